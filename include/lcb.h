@@ -1,0 +1,193 @@
+/*
+ * lcb.h -- C ABI of liblcb.so, the B200 (sm_100a) kernels of the quasistatic
+ * 3D xi step of lcodePy.
+ *
+ * Conventions
+ *  - Every pointer argument is a device pointer unless stated otherwise.
+ *    All arrays are C-ordered (row-major); grids are N x N with the flat
+ *    index  y + N * x  (x = first axis), as in the reference
+ *    (lcode/plasma3d/weights.py:180).  Plasma particle arrays of all sorts
+ *    are concatenated: sort s occupies [s * n_per_sort, (s+1) * n_per_sort).
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default).
+ *  - Every call is asynchronous on `stream` and returns LCB_OK or an error
+ *    code; lcb_last_error() gives a message for the calling thread.
+ *  - `err` (may be NULL) is a device int32 that kernels OR error bits into
+ *    (LCB_DEVERR_*).  The host reads it at its own sync points.
+ *  - The library allocates no device memory: scratch is passed in by the
+ *    caller, with its size given by the matching *_workspace_bytes query.
+ *
+ * Reference interfaces replaced (paths relative to the lcodePy project root)
+ * are cited beside each entry point.
+ */
+#ifndef LCB_H
+#define LCB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LCB_OK 0
+#define LCB_ERR_INVALID 1   /* bad argument (size, pointer, alignment) */
+#define LCB_ERR_CUDA 2      /* a CUDA runtime call failed */
+#define LCB_ERR_DEVICE 3    /* a device error word was found set */
+
+/* Device error bits. */
+#define LCB_DEVERR_PLASMA_STENCIL 1  /* plasma stencil left the grid (NaN or runaway) */
+#define LCB_DEVERR_BEAM_STENCIL 2    /* beam stencil left the N*N array */
+#define LCB_DEVERR_CAPACITY 4        /* a device-side buffer would overflow */
+
+/* Precision modes for the field solver and deposition. */
+#define LCB_PREC_FP64 0   /* FP64 everywhere: the reference's arithmetic */
+#define LCB_PREC_MIXED 1  /* FP32 deposition and FP32 transforms; FP64 particles */
+
+const char *lcb_last_error(void);
+int lcb_version(void);
+/* Number of kernel launches issued by this library since load (all threads). */
+int64_t lcb_launch_count(void);
+
+/* ---------------------------------------------------------------------
+ * Plasma particles
+ * ------------------------------------------------------------------- */
+
+/* Copy prev -> full and free-stream the offsets:
+ *   full = prev;  where m != 0:  x_offt += px / (gamma m - pz) * xi_step.
+ * Replaces move_particles_wo_fields, lcode/plasma3d/move.py:331-349
+ * (the copy) with the kernel move_wo_fields_cupy, move.py:292-313.
+ * prev and full may alias (then it is the in-place kernel alone). */
+int lcb_plasma_move_wo_fields(int64_t n, double xi_step, const double *m,
+                              const double *x_offt_prev, const double *y_offt_prev,
+                              const double *px_prev, const double *py_prev,
+                              const double *pz_prev, const double *q_prev,
+                              double *x_offt_full, double *y_offt_full,
+                              double *px_full, double *py_full, double *pz_full,
+                              double *q_full, void *stream);
+
+/* Fused midpoint field gather and momentum/position update with reflection
+ * at +-boundary and absorption (q_full := 0).  Fields are N x N planes.
+ * Replaces move_smart_cupy, lcode/plasma3d/move.py:169-289, driven by
+ * move_particles_smart, move.py:351-381. */
+int lcb_plasma_move_smart(int64_t n, double xi_step, double boundary, double h,
+                          int grid_steps, const double *Ex, const double *Ey,
+                          const double *Ez, const double *Bx, const double *By,
+                          const double *Bz, const double *x_init,
+                          const double *y_init, const double *x_offt_prev,
+                          const double *y_offt_prev, const double *px_prev,
+                          const double *py_prev, const double *pz_prev,
+                          const double *m, double *q_full, double *x_offt_full,
+                          double *y_offt_full, double *px_full, double *py_full,
+                          double *pz_full, int *err, void *stream);
+
+/* Charge and current deposition of all sorts.  Outputs ro, jx, jy, jz are
+ * (2, N, N) planes (plane s = sort s), zeroed here first.  When ro_initial
+ * is not NULL (background ions) plane 1 of ro is set to it afterwards.
+ * precision LCB_PREC_MIXED accumulates in FP32 and converts to FP64.
+ * Replaces compute_rhoj, lcode/plasma3d/rhoj.py:11-20, with deposit_plasma,
+ * weights.py:249-285, and its kernel deposit_plasma_cupy, weights.py:151-190. */
+int lcb_plasma_deposit(int64_t n_per_sort, int n_sorts, int grid_steps,
+                       double h, int particles_side, int precision,
+                       const double *x_init, const double *y_init,
+                       const double *x_offt, const double *y_offt,
+                       const double *px, const double *py, const double *pz,
+                       const double *q, const double *m, const double *ro_initial,
+                       double *ro, double *jx, double *jy, double *jz,
+                       void *workspace, size_t workspace_bytes, int *err,
+                       void *stream);
+size_t lcb_plasma_deposit_workspace_bytes(int grid_steps, int precision);
+
+/* ---------------------------------------------------------------------
+ * Field solver
+ * ------------------------------------------------------------------- */
+
+/* Constant operators, built once on the host and uploaded (FP64):
+ *   dst  (N-2)x(N-2): 2 sin(pi (j+1)(k+1) / (N-1))        DST-I
+ *   dct  N x N      : c_j cos(pi j k / (N-1)), c = 1,2..2,1 DCT-I (rows k)
+ *   dctT N x N      : its transpose
+ *   dirichlet (N-2)^2, mixed (N-2)xN, mixedT Nx(N-2), neumann NxN: the
+ *   reference's solver matrices (lcode/plasma3d/initialization.py:15-67).
+ * For LCB_PREC_MIXED the same operators are also given in FP32 (the *_f
+ * pointers); they may be NULL in FP64 mode. */
+typedef struct lcb_field_consts {
+    const double *dst, *dct, *dctT;
+    const double *dirichlet, *mixed, *mixedT, *neumann;
+    const float *dst_f, *dct_f, *dctT_f;
+    const float *dirichlet_f, *mixed_f, *mixedT_f, *neumann_f;
+} lcb_field_consts;
+
+/* Seven N x N planes in the order Ex, Ey, Ez, Bx, By, Bz, Phi. */
+typedef struct lcb_fields {
+    double *f[7];
+} lcb_fields;
+
+/* Currents: four (n_planes, N, N) arrays ro, jx, jy, jz. */
+typedef struct lcb_currents {
+    const double *ro, *jx, *jy, *jz;
+    int n_planes;
+} lcb_currents;
+
+typedef struct lcb_compute_fields_args {
+    int grid_steps;
+    double h, xi_step, subtraction_coeff;
+    int precision;
+    lcb_field_consts consts;
+    lcb_fields fields;       /* Ex, Ey, Bx, By read (Helmholtz term) */
+    lcb_fields fields_prev;  /* read */
+    lcb_currents currents_prev, currents_full;
+    const double *rho_beam_full, *rho_beam_prev; /* N x N */
+    double rho_beam_divisor;  /* beam planes are divided by this (h^2 or 1) */
+    lcb_fields out_full;      /* written; any plane may be NULL (skipped) */
+    lcb_fields out_half;      /* written; any plane may be NULL */
+    void *workspace;
+    size_t workspace_bytes;
+} lcb_compute_fields_args;
+
+/* Replaces compute_fields, lcode/plasma3d/fields.py:276-322 (with
+ * calculate_Ex_Ey_Bx_By :176-230, calculate_Ez :112-139, calculate_Bz
+ * :233-266, calculate_Phi :142-159 and the GPU transforms :36-107): every
+ * DST-I / DCT-I / mixed transform is a dense batched matrix product. */
+int lcb_compute_fields(const lcb_compute_fields_args *a, void *stream);
+size_t lcb_compute_fields_workspace_bytes(int grid_steps, int precision);
+
+/* ---------------------------------------------------------------------
+ * Beam
+ * ------------------------------------------------------------------- */
+
+/* Beam density: 25-point transverse x linear-in-xi deposit of a layer into
+ * the carried plane ro0 (weight xi_loc) and the next plane ro1 (1 - xi_loc),
+ * xi_loc = (-xi_step * layer_idx - xi) / xi_step.  Accumulates (no zeroing).
+ * Replaces deposit_beam, lcode/beam3d/weights.py:152-163, and its kernel
+ * deposit_beam_cupy, weights.py:108-138. */
+int lcb_beam_deposit(int64_t n, int grid_steps, double h, double xi_step,
+                     int64_t layer_idx, const double *x, const double *y,
+                     const double *xi, const double *q_norm, double *ro0,
+                     double *ro1, int *err, void *stream);
+
+/* Substep sizes for the first n_fresh particles of a layer:
+ *   d = 1, halved while d > sqrt(sqrt(1/q_m^2 + pz^2) / substep_energy);
+ *   dt = d * time_step; remaining_steps = (int64)(1 / d).
+ * Replaces start_moving_layer with calculate_substepping_step,
+ * lcode/beam3d/beam_calculator.py:28-46,97-114. */
+int lcb_beam_substepping(int64_t n_fresh, const double *q_m, const double *pz,
+                         double substep_energy, double time_step, double *dt,
+                         int64_t *remaining_steps, void *stream);
+
+/* Substepped Higuera-Cary push of a layer between plane k (fields_k,
+ * = previous xi step) and plane k+1 (fields_k1, = new xi step).  Writes
+ * flags[i] = 1 lost | 2 moved | 4 fell.
+ * Replaces move_beam_layer, lcode/beam3d/beam_calculator.py:116-134, with
+ * the kernel move_beam_cupy, lcode/beam3d/move.py:132-276. */
+int lcb_beam_move(int64_t n, double xi_step, double r_max,
+                  int64_t beam_layer_idx, double h, int grid_steps,
+                  const double *q_m, const double *dt,
+                  const lcb_fields *fields_k, const lcb_fields *fields_k1,
+                  int64_t *remaining_steps, int64_t *id, double *x, double *y,
+                  double *xi, double *px, double *py, double *pz,
+                  uint8_t *flags, int *err, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LCB_H */

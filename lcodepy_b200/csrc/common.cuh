@@ -1,0 +1,62 @@
+// Shared device helpers for liblcb (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "../../include/lcb.h"
+
+namespace lcb {
+
+// ---- error reporting (host) ----
+void set_error(const char *fmt, ...);
+int cuda_check(cudaError_t e, const char *what);
+void count_launch(int n = 1);
+
+#define LCB_LAUNCH_CHECK(what)                                              \
+    do {                                                                    \
+        ::lcb::count_launch();                                              \
+        cudaError_t _e = cudaGetLastError();                                \
+        if (_e != cudaSuccess) return ::lcb::cuda_check(_e, what);          \
+    } while (0)
+
+#define LCB_REQUIRE(cond, ...)                                              \
+    do {                                                                    \
+        if (!(cond)) { ::lcb::set_error(__VA_ARGS__); return LCB_ERR_INVALID; } \
+    } while (0)
+
+inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Number of SMs of the current device (cached per process; one device per
+// process is the deployment model).
+int sm_count();
+
+// ---- 4th-order spline weights at offsets -2..2 ----
+// The reference's weight4 (lcode/plasma3d/weights.py:13-31, :127-148),
+// evaluated for all five offsets at once.
+__device__ __forceinline__ void weights4(double x, double w[5])
+{
+    const double x2 = x * x, x3 = x2 * x, x4 = x3 * x;
+    const double a = 0.5 - x, b = 0.5 + x;
+    w[0] = a * a * a * a / 24.;
+    w[1] = 19 / 96. - 11 / 24. * x + x2 / 4. + x3 / 6. - x4 / 6.;
+    w[2] = 115 / 192. - 5 / 8. * x2 + x4 / 4.;
+    w[3] = 19 / 96. + 11 / 24. * x + x2 / 4. - x3 / 6. - x4 / 6.;
+    w[4] = b * b * b * b / 24.;
+}
+
+// Cell of a position (in cell units, already offset by +0.5) and the local
+// coordinate in [-0.5, 0.5): the reference's
+//   x_loc = x_h - floor(x_h) - 0.5;  ix = floor(x_h) + floor(N / 2).
+__device__ __forceinline__ int cell_of(double x_h, int half_n, double &loc)
+{
+    const double f = floor(x_h);
+    loc = x_h - f - 0.5;
+    // Values far outside the grid (or NaN) must not overflow the int cast;
+    // clamp to a sentinel the caller's bounds check rejects.
+    if (!(f > -1e9 && f < 1e9)) return INT32_MIN / 2;
+    return (int)f + half_n;
+}
+
+}  // namespace lcb

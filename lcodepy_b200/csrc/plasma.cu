@@ -1,0 +1,365 @@
+// Plasma particle kernels: free-streaming estimate, fused gather + push, and
+// tiled charge/current deposition.  FP64 particles (SoA, coalesced).
+#include "common.cuh"
+
+namespace lcb {
+
+// ---------------------------------------------------------------------------
+// K1: copy prev -> full and free-stream (lcode/plasma3d/move.py:292-313,
+// copy at :337-339).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+k_move_wo_fields(int64_t n, double xi_step, const double *__restrict__ m,
+                 const double *__restrict__ xo_p, const double *__restrict__ yo_p,
+                 const double *__restrict__ px_p, const double *__restrict__ py_p,
+                 const double *__restrict__ pz_p, const double *__restrict__ q_p,
+                 double *xo_f, double *yo_f, double *px_f, double *py_f,
+                 double *pz_f, double *q_f)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const double mk = m[k], px = px_p[k], py = py_p[k], pz = pz_p[k];
+        double xo = xo_p[k], yo = yo_p[k];
+        if (mk != 0) {
+            const double gm = sqrt(mk * mk + pz * pz + px * px + py * py);
+            xo += px / (gm - pz) * xi_step;
+            yo += py / (gm - pz) * xi_step;
+        }
+        xo_f[k] = xo; yo_f[k] = yo;
+        px_f[k] = px; py_f[k] = py; pz_f[k] = pz;
+        q_f[k] = q_p[k];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// K2: fused midpoint gather + two-pass momentum update + advance +
+// reflection + absorption (lcode/plasma3d/move.py:169-289).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void reflect(double &x, double b, double &px, double &py, double &pz)
+{
+    if (x > b)  { x =  2 * b - x; px = py = pz = 0; }
+    if (x < -b) { x = -2 * b - x; px = py = pz = 0; }
+}
+
+__global__ void __launch_bounds__(256)
+k_move_smart(int64_t n, double xi_step, double boundary, double h, int N,
+             const double *__restrict__ Exf, const double *__restrict__ Eyf,
+             const double *__restrict__ Ezf, const double *__restrict__ Bxf,
+             const double *__restrict__ Byf, const double *__restrict__ Bzf,
+             const double *__restrict__ x_init, const double *__restrict__ y_init,
+             const double *__restrict__ xo_p, const double *__restrict__ yo_p,
+             const double *__restrict__ px_p, const double *__restrict__ py_p,
+             const double *__restrict__ pz_p, const double *__restrict__ m,
+             double *q_f, double *xo_f, double *yo_f, double *px_f,
+             double *py_f, double *pz_f, int *err)
+{
+    const int half_n = N / 2;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const double qk = q_f[k];
+        if (qk == 0) continue;
+        const double xi0 = x_init[k], yi0 = y_init[k];
+        const double opx = px_p[k], opy = py_p[k], opz = pz_p[k];
+        double px = opx, py = opy, pz = opz;
+        double xh = xi0 + (xo_p[k] + xo_f[k]) / 2;
+        double yh = yi0 + (yo_p[k] + yo_f[k]) / 2;
+        // The reference zeroes momenta when the midpoint is reflected; the
+        // zeroed values only feed gamma in the first pass below.
+        if (xh > boundary)  { xh =  2 * boundary - xh; px = py = pz = 0; }
+        if (xh < -boundary) { xh = -2 * boundary - xh; px = py = pz = 0; }
+        if (yh > boundary)  { yh =  2 * boundary - yh; px = py = pz = 0; }
+        if (yh < -boundary) { yh = -2 * boundary - yh; px = py = pz = 0; }
+
+        double xl, yl;
+        const int ix = cell_of(xh / h + 0.5, half_n, xl);
+        const int iy = cell_of(yh / h + 0.5, half_n, yl);
+        double Ex = 0, Ey = 0, Ez = 0, Bx = 0, By = 0, Bz = 0;
+        if (ix >= 2 && ix < N - 2 && iy >= 2 && iy < N - 2) {
+            double wx[5], wy[5];
+            weights4(xl, wx);
+            weights4(yl, wy);
+#pragma unroll
+            for (int a = 0; a < 5; a++) {
+                const int row = (ix + a - 2) * N + iy - 2;
+#pragma unroll
+                for (int b = 0; b < 5; b++) {
+                    const double w = wx[a] * wy[b];
+                    const int idx = row + b;
+                    Ex += __ldg(Exf + idx) * w; Bx += __ldg(Bxf + idx) * w;
+                    Ey += __ldg(Eyf + idx) * w; By += __ldg(Byf + idx) * w;
+                    Ez += __ldg(Ezf + idx) * w; Bz += __ldg(Bzf + idx) * w;
+                }
+            }
+        } else if (err) {
+            atomicOr(err, LCB_DEVERR_PLASMA_STENCIL);
+        }
+        const double mk = m[k];
+        double gm = sqrt(mk * mk + px * px + py * py + pz * pz);
+        double vx = px / gm, vy = py / gm, vz = pz / gm;
+        double f = qk * xi_step / (1 - pz / gm);
+        double dpx = f * (Ex + vy * Bz - vz * By);
+        double dpy = f * (Ey - vx * Bz + vz * Bx);
+        double dpz = f * (Ez + vx * By - vy * Bx);
+        px = opx + dpx / 2; py = opy + dpy / 2; pz = opz + dpz / 2;
+
+        gm = sqrt(mk * mk + px * px + py * py + pz * pz);
+        vx = px / gm; vy = py / gm; vz = pz / gm;
+        f = qk * xi_step / (1 - pz / gm);
+        dpx = f * (Ex + vy * Bz - vz * By);
+        dpy = f * (Ey - vx * Bz + vz * Bx);
+        dpz = f * (Ez + vx * By - vy * Bx);
+        px = opx + dpx / 2; py = opy + dpy / 2; pz = opz + dpz / 2;
+
+        gm = sqrt(mk * mk + px * px + py * py + pz * pz);
+        double xo = xo_p[k] + px / (gm - pz) * xi_step;
+        double yo = yo_p[k] + py / (gm - pz) * xi_step;
+        px = opx + dpx; py = opy + dpy; pz = opz + dpz;
+
+        double x = xi0 + xo, y = yi0 + yo;
+        if (x > boundary)  { x =  2 * boundary - x; xo = x - xi0; px = py = pz = 0; }
+        if (x < -boundary) { x = -2 * boundary - x; xo = x - xi0; px = py = pz = 0; }
+        if (y > boundary)  { y =  2 * boundary - y; yo = y - yi0; px = py = pz = 0; }
+        if (y < -boundary) { y = -2 * boundary - y; yo = y - yi0; px = py = pz = 0; }
+        if (x >= boundary || x <= -boundary || y >= boundary || y <= -boundary) {
+            xo = yo = 0; px = py = pz = 0;
+            q_f[k] = 0;
+        }
+        xo_f[k] = xo; yo_f[k] = yo;
+        px_f[k] = px; py_f[k] = py; pz_f[k] = pz;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// K3: deposition (lcode/plasma3d/weights.py:151-190, 249-285).
+//
+// A block owns a TI x TJ tile of one sort's particle lattice (particles are
+// created on a lattice, k = s*Np + i*Ns + j, and drift little per xi step, so
+// a tile's particles stay in a compact cell window).  Contributions whose
+// whole 5x5 stencil lies inside the block's shared-memory window [wx0, wx0+WX)
+// x [wy0, wy0+WY) are accumulated there with shared atomics; any other
+// particle (a runaway, a lattice that is not a lattice) goes straight to
+// global atomics.  The window is then flushed with one global atomic per
+// non-zero cell and quantity.  The window origin follows the tile's first
+// particle's *initial* position, with S cells of slack for drift.
+// ---------------------------------------------------------------------------
+constexpr int DEP_TI = 16, DEP_TJ = 32, DEP_THREADS = 256;
+constexpr int DEP_SLACK = 4;
+constexpr int DEP_WX = 28, DEP_WY = 44;  // >= tile cells (fineness 1) + 4 + 2*slack
+
+template <typename Acc>
+__global__ void __launch_bounds__(DEP_THREADS)
+k_deposit_tiled(int64_t n_per_sort, int Ns, int N, double h,
+                const double *__restrict__ x_init, const double *__restrict__ y_init,
+                const double *__restrict__ x_offt, const double *__restrict__ y_offt,
+                const double *__restrict__ px_a, const double *__restrict__ py_a,
+                const double *__restrict__ pz_a, const double *__restrict__ q_a,
+                const double *__restrict__ m_a, Acc *ro, Acc *jx, Acc *jy, Acc *jz,
+                int *err)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Acc *sw = reinterpret_cast<Acc *>(smem_raw);  // [4][WX][WY]
+    constexpr int WSZ = DEP_WX * DEP_WY;
+    const int s = blockIdx.z;
+    const int i0 = blockIdx.y * DEP_TI, j0 = blockIdx.x * DEP_TJ;
+    const int64_t base = (int64_t)s * n_per_sort;
+    const int half_n = N / 2;
+    const int64_t NN = (int64_t)N * N;
+    Acc *gro = ro + s * NN, *gjx = jx + s * NN, *gjy = jy + s * NN, *gjz = jz + s * NN;
+
+    for (int t = threadIdx.x; t < 4 * WSZ; t += blockDim.x) sw[t] = Acc(0);
+    // window origin from the tile's first particle's initial lattice position
+    double dummy;
+    const int64_t k0 = base + (int64_t)i0 * Ns + j0;
+    const int wx0 = cell_of(x_init[k0] / h + 0.5, half_n, dummy) - 2 - DEP_SLACK;
+    const int wy0 = cell_of(y_init[k0] / h + 0.5, half_n, dummy) - 2 - DEP_SLACK;
+    __syncthreads();
+
+    const int tj = threadIdx.x % DEP_TJ;
+    for (int ti = threadIdx.x / DEP_TJ; ti < DEP_TI; ti += DEP_THREADS / DEP_TJ) {
+        const int i = i0 + ti, j = j0 + tj;
+        if (i >= Ns || j >= Ns) continue;
+        const int64_t k = base + (int64_t)i * Ns + j;
+        const double q = q_a[k];
+        if (q == 0) continue;
+        const double m = m_a[k], px = px_a[k], py = py_a[k], pz = pz_a[k];
+        const double gm = sqrt(m * m + px * px + py * py + pz * pz);
+        const double dro = q / (1 - pz / gm);
+        const double djx = px * (dro / gm), djy = py * (dro / gm), djz = pz * (dro / gm);
+        double xl, yl;
+        const int ix = cell_of((x_init[k] + x_offt[k]) / h + 0.5, half_n, xl);
+        const int iy = cell_of((y_init[k] + y_offt[k]) / h + 0.5, half_n, yl);
+        if (!(ix >= 2 && ix < N - 2 && iy >= 2 && iy < N - 2)) {
+            if (err) atomicOr(err, LCB_DEVERR_PLASMA_STENCIL);
+            continue;
+        }
+        double wx[5], wy[5];
+        weights4(xl, wx);
+        weights4(yl, wy);
+        const int lx = ix - 2 - wx0, ly = iy - 2 - wy0;
+        if (lx >= 0 && lx + 5 <= DEP_WX && ly >= 0 && ly + 5 <= DEP_WY) {
+#pragma unroll
+            for (int a = 0; a < 5; a++) {
+                const double wxa = wx[a] / h;
+#pragma unroll
+                for (int b = 0; b < 5; b++) {
+                    const double w = wxa * wy[b] / h;
+                    const int c = (lx + a) * DEP_WY + ly + b;
+                    atomicAdd(sw + c, Acc(dro * w));
+                    atomicAdd(sw + WSZ + c, Acc(djx * w));
+                    atomicAdd(sw + 2 * WSZ + c, Acc(djy * w));
+                    atomicAdd(sw + 3 * WSZ + c, Acc(djz * w));
+                }
+            }
+        } else {
+#pragma unroll
+            for (int a = 0; a < 5; a++) {
+                const double wxa = wx[a] / h;
+#pragma unroll
+                for (int b = 0; b < 5; b++) {
+                    const double w = wxa * wy[b] / h;
+                    const int64_t c = (int64_t)(ix + a - 2) * N + iy + b - 2;
+                    atomicAdd(gro + c, Acc(dro * w));
+                    atomicAdd(gjx + c, Acc(djx * w));
+                    atomicAdd(gjy + c, Acc(djy * w));
+                    atomicAdd(gjz + c, Acc(djz * w));
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < WSZ; t += blockDim.x) {
+        const int gx = wx0 + t / DEP_WY, gy = wy0 + t % DEP_WY;
+        if (gx < 0 || gx >= N || gy < 0 || gy >= N) continue;
+        const int64_t c = (int64_t)gx * N + gy;
+        const Acc v0 = sw[t], v1 = sw[WSZ + t], v2 = sw[2 * WSZ + t], v3 = sw[3 * WSZ + t];
+        if (v0 != Acc(0)) atomicAdd(gro + c, v0);
+        if (v1 != Acc(0)) atomicAdd(gjx + c, v1);
+        if (v2 != Acc(0)) atomicAdd(gjy + c, v2);
+        if (v3 != Acc(0)) atomicAdd(gjz + c, v3);
+    }
+}
+
+__global__ void k_f32_to_f64(int64_t n, const float *__restrict__ a, double *__restrict__ b)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (double)a[i];
+}
+
+static int grid_for(int64_t n, int threads)
+{
+    int64_t blocks = (n + threads - 1) / threads;
+    const int64_t cap = (int64_t)sm_count() * 16;
+    if (blocks > cap) blocks = cap;
+    return (int)(blocks < 1 ? 1 : blocks);
+}
+
+}  // namespace lcb
+
+using namespace lcb;
+
+extern "C" int lcb_plasma_move_wo_fields(
+    int64_t n, double xi_step, const double *m, const double *x_offt_prev,
+    const double *y_offt_prev, const double *px_prev, const double *py_prev,
+    const double *pz_prev, const double *q_prev, double *x_offt_full,
+    double *y_offt_full, double *px_full, double *py_full, double *pz_full,
+    double *q_full, void *stream)
+{
+    LCB_REQUIRE(n >= 0, "n < 0");
+    if (n == 0) return LCB_OK;
+    k_move_wo_fields<<<grid_for(n, 256), 256, 0, as_stream(stream)>>>(
+        n, xi_step, m, x_offt_prev, y_offt_prev, px_prev, py_prev, pz_prev,
+        q_prev, x_offt_full, y_offt_full, px_full, py_full, pz_full, q_full);
+    LCB_LAUNCH_CHECK("k_move_wo_fields");
+    return LCB_OK;
+}
+
+extern "C" int lcb_plasma_move_smart(
+    int64_t n, double xi_step, double boundary, double h, int grid_steps,
+    const double *Ex, const double *Ey, const double *Ez, const double *Bx,
+    const double *By, const double *Bz, const double *x_init,
+    const double *y_init, const double *x_offt_prev, const double *y_offt_prev,
+    const double *px_prev, const double *py_prev, const double *pz_prev,
+    const double *m, double *q_full, double *x_offt_full, double *y_offt_full,
+    double *px_full, double *py_full, double *pz_full, int *err, void *stream)
+{
+    LCB_REQUIRE(n >= 0 && grid_steps >= 5, "bad sizes n=%lld N=%d", (long long)n, grid_steps);
+    if (n == 0) return LCB_OK;
+    k_move_smart<<<grid_for(n, 256), 256, 0, as_stream(stream)>>>(
+        n, xi_step, boundary, h, grid_steps, Ex, Ey, Ez, Bx, By, Bz, x_init,
+        y_init, x_offt_prev, y_offt_prev, px_prev, py_prev, pz_prev, m, q_full,
+        x_offt_full, y_offt_full, px_full, py_full, pz_full, err);
+    LCB_LAUNCH_CHECK("k_move_smart");
+    return LCB_OK;
+}
+
+extern "C" size_t lcb_plasma_deposit_workspace_bytes(int grid_steps, int precision)
+{
+    if (precision == LCB_PREC_MIXED)
+        return (size_t)8 * grid_steps * grid_steps * sizeof(float);
+    return 0;
+}
+
+extern "C" int lcb_plasma_deposit(
+    int64_t n_per_sort, int n_sorts, int grid_steps, double h, int particles_side,
+    int precision, const double *x_init, const double *y_init,
+    const double *x_offt, const double *y_offt, const double *px,
+    const double *py, const double *pz, const double *q, const double *m,
+    const double *ro_initial, double *ro, double *jx, double *jy, double *jz,
+    void *workspace, size_t workspace_bytes, int *err, void *stream)
+{
+    const int N = grid_steps;
+    LCB_REQUIRE(n_sorts >= 1 && n_sorts <= 2, "n_sorts must be 1 or 2");
+    LCB_REQUIRE((int64_t)particles_side * particles_side == n_per_sort,
+                "n_per_sort (%lld) must be particles_side^2 (%d^2)",
+                (long long)n_per_sort, particles_side);
+    LCB_REQUIRE(N >= 5, "grid_steps < 5");
+    LCB_REQUIRE(precision == LCB_PREC_FP64 || precision == LCB_PREC_MIXED, "bad precision");
+    cudaStream_t st = as_stream(stream);
+    const size_t plane = (size_t)N * N;
+    const size_t bytes = 2 * plane * sizeof(double);
+    for (double *p : {ro, jx, jy, jz}) {
+        cudaError_t e = cudaMemsetAsync(p, 0, bytes, st);
+        if (e != cudaSuccess) return cuda_check(e, "memset currents");
+    }
+    if (n_per_sort > 0) {
+        dim3 grid((particles_side + DEP_TJ - 1) / DEP_TJ,
+                  (particles_side + DEP_TI - 1) / DEP_TI, n_sorts);
+        if (precision == LCB_PREC_FP64) {
+            const size_t sm = 4 * DEP_WX * DEP_WY * sizeof(double);
+            static bool attr = false;
+            if (!attr) {
+                cudaFuncSetAttribute(k_deposit_tiled<double>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+                attr = true;
+            }
+            k_deposit_tiled<double><<<grid, DEP_THREADS, sm, st>>>(
+                n_per_sort, particles_side, N, h, x_init, y_init, x_offt, y_offt,
+                px, py, pz, q, m, ro, jx, jy, jz, err);
+            LCB_LAUNCH_CHECK("k_deposit_tiled<double>");
+        } else {
+            LCB_REQUIRE(workspace && workspace_bytes >= lcb_plasma_deposit_workspace_bytes(N, precision),
+                        "deposit workspace too small");
+            float *w = static_cast<float *>(workspace);
+            cudaError_t e = cudaMemsetAsync(w, 0, 8 * plane * sizeof(float), st);
+            if (e != cudaSuccess) return cuda_check(e, "memset f32 currents");
+            const size_t sm = 4 * DEP_WX * DEP_WY * sizeof(float);
+            k_deposit_tiled<float><<<grid, DEP_THREADS, sm, st>>>(
+                n_per_sort, particles_side, N, h, x_init, y_init, x_offt, y_offt,
+                px, py, pz, q, m, w, w + 2 * plane, w + 4 * plane, w + 6 * plane, err);
+            LCB_LAUNCH_CHECK("k_deposit_tiled<float>");
+            const int64_t cnt = (int64_t)2 * plane;
+            double *outs[4] = {ro, jx, jy, jz};
+            for (int qd = 0; qd < 4; qd++) {
+                k_f32_to_f64<<<grid_for(cnt, 256), 256, 0, st>>>(cnt, w + qd * 2 * plane, outs[qd]);
+                LCB_LAUNCH_CHECK("k_f32_to_f64");
+            }
+        }
+    }
+    if (ro_initial) {
+        cudaError_t e = cudaMemcpyAsync(ro + plane, ro_initial, plane * sizeof(double),
+                                        cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return cuda_check(e, "copy ro_initial");
+    }
+    return LCB_OK;
+}

@@ -1,0 +1,232 @@
+"""Device-resident plasma xi step (lcode/plasma3d/solver.py:25-78).
+
+``Plane2d3vPlasmaSolver`` owns every device buffer of the plasma response and
+advances it by one xi step through liblcb.so:
+
+    K1 move_wo_fields -> K2 move_smart(fields_prev) -> K3 deposit
+      -> compute_fields(fields_prev)          -> half A
+      -> K2(half A) -> K3 -> compute_fields(half A) -> full, half B
+      -> K2(half B) -> K3
+
+Buffers rotate instead of being copied: particles (prev, full), fields
+(prev, full) and currents (prev, full) swap roles after each step.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from .config import Config
+from .data import Arrays
+from .plasma3d import (CURRENT_NAMES, FIELD_NAMES, FieldOperators, PlasmaState,
+                       host_initial_particles, plasma_params, sorts_of)
+
+
+class FieldSet:
+    """Seven N x N FP64 planes."""
+
+    def __init__(self, N, device):
+        self.buf = torch.zeros(7, N, N, dtype=torch.float64, device=device)
+        self.struct = _lib.Fields7()
+        for i in range(7):
+            self.struct.f[i] = self.buf[i].data_ptr()
+
+    def __getattr__(self, k):
+        if k in FIELD_NAMES:
+            return self.__dict__["buf"][FIELD_NAMES.index(k)]
+        raise AttributeError(k)
+
+    def arrays(self) -> Arrays:
+        return Arrays(torch, **{k: self.buf[i] for i, k in enumerate(FIELD_NAMES)})
+
+
+class CurrentSet:
+    """ro, jx, jy, jz, each (2, N, N)."""
+
+    def __init__(self, N, device):
+        self.buf = torch.zeros(4, 2, N, N, dtype=torch.float64, device=device)
+        self.struct = _lib.Currents4(*(self.buf[i].data_ptr() for i in range(4)), 2)
+
+    def __getattr__(self, k):
+        if k in CURRENT_NAMES:
+            return self.__dict__["buf"][CURRENT_NAMES.index(k)]
+        raise AttributeError(k)
+
+    def arrays(self) -> Arrays:
+        return Arrays(torch, **{k: self.buf[i] for i, k in enumerate(CURRENT_NAMES)})
+
+
+class Plane2d3vPlasmaSolver:
+    """The plasma response to one xi step, on the GPU."""
+
+    def __init__(self, config: Config, device=None):
+        if config.getbool('declustering-enabled'):
+            raise NotImplementedError("declustering (noise filter) is not supported")
+        self.device = device or torch.device("cuda", torch.cuda.current_device())
+        self.config = config
+        p = plasma_params(config)
+        self.N, self.h, self.dxi = p["N"], p["h"], p["dxi"]
+        self.boundary, self.sub_coeff = p["boundary"], p["sub_coeff"]
+        self.ion_model, self.precision = p["ion_model"], p["precision"]
+        self.sort_names = sorts_of(self.ion_model)
+        self.n_sorts = len(self.sort_names)
+        _lib.load()
+        self.ops = FieldOperators(self.N, self.h, self.sub_coeff, self.device,
+                                  self.precision == _lib.LCB_PREC_MIXED)
+        N, dev = self.N, self.device
+        self.fields = [FieldSet(N, dev) for _ in range(2)]   # prev, full (rotating)
+        self.half = [FieldSet(N, dev) for _ in range(2)]     # half A, half B
+        self.currents = [CurrentSet(N, dev) for _ in range(2)]
+        self.ws_fields = torch.empty(
+            _lib.load().lcb_compute_fields_workspace_bytes(N, self.precision),
+            dtype=torch.uint8, device=dev)
+        ws_dep = _lib.load().lcb_plasma_deposit_workspace_bytes(N, self.precision)
+        self.ws_dep = torch.empty(max(ws_dep, 256), dtype=torch.uint8, device=dev)
+        self.err = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.ro_initial = torch.zeros(N, N, dtype=torch.float64, device=dev)
+        self.zero_plane = torch.zeros(N, N, dtype=torch.float64, device=dev)
+        self.states = None
+        self.cur = 0  # index of the "prev" copy in self.states / fields / currents
+
+    # -- initial state (initialization.py:278-414) --
+    def init_state(self, current_time=0.0):
+        x_init, y_init, q, m = host_initial_particles(self.config, current_time)
+        Ns = x_init.shape[0]
+        dev = self.device
+        if self.states is None or self.states[0].Ns != Ns:
+            self.states = [PlasmaState(self.n_sorts, Ns, dev) for _ in range(2)]
+        st = self.states[0]
+        n = Ns * Ns
+        xi_t = torch.from_numpy(x_init.ravel()).to(dev)
+        yi_t = torch.from_numpy(y_init.ravel()).to(dev)
+        q_t = torch.from_numpy(q.ravel()).to(dev)
+        m_t = torch.from_numpy(m.ravel()).to(dev)
+        for s in (self.states[0], self.states[1]):
+            for k in ("x_offt", "y_offt", "px", "py", "pz"):
+                s.t[k].zero_()
+            for si in range(self.n_sorts):
+                sl = slice(si * n, (si + 1) * n)
+                s.x_init[sl] = xi_t
+                s.y_init[sl] = yi_t
+            s.q[:n] = q_t
+            s.m[:n] = m_t
+            if self.n_sorts == 2:
+                s.q[n:] = -q_t
+                s.m[n:] = self.config.getfloat("ion-mass") * m_t
+        # background charge: minus the deposited initial electrons
+        # (initialization.py:351-356)
+        tmp = self.currents[1]
+        self._deposit(st, tmp, with_background=False, n_sorts=1)
+        self.ro_initial.copy_(-tmp.ro[0])
+        for f in self.fields + self.half:
+            f.buf.zero_()
+        for c in self.currents:
+            c.buf.zero_()
+        self.err.zero_()
+        self.cur = 0
+
+    # -- kernels --
+    def _deposit(self, st: PlasmaState, out: CurrentSet, with_background=True, n_sorts=None):
+        L = _lib.load()
+        n_sorts = n_sorts or self.n_sorts
+        bg = self.ro_initial if (with_background and self.ion_model == "background") else None
+        _lib.check(L.lcb_plasma_deposit(
+            st.n_per_sort, n_sorts, self.N, self.h, st.Ns, self.precision,
+            st.x_init.data_ptr(), st.y_init.data_ptr(), st.x_offt.data_ptr(),
+            st.y_offt.data_ptr(), st.px.data_ptr(), st.py.data_ptr(), st.pz.data_ptr(),
+            st.q.data_ptr(), st.m.data_ptr(), _lib.ptr(bg),
+            out.ro.data_ptr(), out.jx.data_ptr(), out.jy.data_ptr(), out.jz.data_ptr(),
+            self.ws_dep.data_ptr(), self.ws_dep.numel(), self.err.data_ptr(),
+            _lib.stream_handle()), "lcb_plasma_deposit")
+
+    def _move_wo_fields(self, prev: PlasmaState, full: PlasmaState):
+        L = _lib.load()
+        _lib.check(L.lcb_plasma_move_wo_fields(
+            prev.x_offt.numel(), self.dxi, prev.m.data_ptr(),
+            prev.x_offt.data_ptr(), prev.y_offt.data_ptr(), prev.px.data_ptr(),
+            prev.py.data_ptr(), prev.pz.data_ptr(), prev.q.data_ptr(),
+            full.x_offt.data_ptr(), full.y_offt.data_ptr(), full.px.data_ptr(),
+            full.py.data_ptr(), full.pz.data_ptr(), full.q.data_ptr(),
+            _lib.stream_handle()), "lcb_plasma_move_wo_fields")
+
+    def _move_smart(self, F: FieldSet, prev: PlasmaState, full: PlasmaState):
+        L = _lib.load()
+        fb = F.buf
+        _lib.check(L.lcb_plasma_move_smart(
+            prev.x_offt.numel(), self.dxi, self.boundary, self.h, self.N,
+            *(fb[i].data_ptr() for i in range(6)),
+            prev.x_init.data_ptr(), prev.y_init.data_ptr(),
+            prev.x_offt.data_ptr(), prev.y_offt.data_ptr(), prev.px.data_ptr(),
+            prev.py.data_ptr(), prev.pz.data_ptr(), full.m.data_ptr(),
+            full.q.data_ptr(), full.x_offt.data_ptr(), full.y_offt.data_ptr(),
+            full.px.data_ptr(), full.py.data_ptr(), full.pz.data_ptr(),
+            self.err.data_ptr(), _lib.stream_handle()), "lcb_plasma_move_smart")
+
+    def _compute_fields(self, F: FieldSet, Fprev: FieldSet, cprev: CurrentSet,
+                        cfull: CurrentSet, rb_full, rb_prev, rb_div,
+                        out_full: FieldSet | None, out_half: FieldSet):
+        a = _lib.ComputeFieldsArgs()
+        a.grid_steps, a.h, a.xi_step = self.N, self.h, self.dxi
+        a.subtraction_coeff, a.precision = self.sub_coeff, self.precision
+        a.consts = self.ops.struct
+        a.fields, a.fields_prev = F.struct, Fprev.struct
+        a.currents_prev, a.currents_full = cprev.struct, cfull.struct
+        a.rho_beam_full, a.rho_beam_prev = rb_full.data_ptr(), rb_prev.data_ptr()
+        a.rho_beam_divisor = rb_div
+        if out_full is not None:
+            a.out_full = out_full.struct
+        a.out_half = out_half.struct
+        a.workspace, a.workspace_bytes = self.ws_fields.data_ptr(), self.ws_fields.numel()
+        _lib.check(_lib.load().lcb_compute_fields(C.byref(a), _lib.stream_handle()),
+                   "lcb_compute_fields")
+
+    # -- the xi step --
+    @property
+    def prev_fields(self) -> FieldSet:
+        return self.fields[self.cur]
+
+    @property
+    def prev_currents(self) -> CurrentSet:
+        return self.currents[self.cur]
+
+    @property
+    def prev_particles(self) -> PlasmaState:
+        return self.states[self.cur]
+
+    def step_dxi(self, rb_full: torch.Tensor, rb_prev: torch.Tensor, rb_div: float = 1.0):
+        """Advance the plasma by one xi step; afterwards the new state is the
+        "prev" state (fields / currents / particles) and the step's input
+        fields remain readable as ``last_fields`` until the next step."""
+        p, f = self.cur, 1 - self.cur
+        prev, full = self.states[p], self.states[f]
+        Fp, Ff = self.fields[p], self.fields[f]
+        cp, cf = self.currents[p], self.currents[f]
+        hA, hB = self.half
+        self._move_wo_fields(prev, full)
+        self._move_smart(Fp, prev, full)
+        self._deposit(full, cf)
+        self._compute_fields(Fp, Fp, cp, cf, rb_full, rb_prev, rb_div, None, hA)
+        self._move_smart(hA, prev, full)
+        self._deposit(full, cf)
+        self._compute_fields(hA, Fp, cp, cf, rb_full, rb_prev, rb_div, Ff, hB)
+        self._move_smart(hB, prev, full)
+        self._deposit(full, cf)
+        self.cur = f
+        self.last_fields = Fp
+
+    # -- views with the reference's names --
+    def particles_dict(self) -> dict:
+        st = self.prev_particles
+        return {name: st.sort_arrays(s) for s, name in enumerate(self.sort_names)}
+
+    def check_errors(self):
+        e = int(self.err.item())
+        if e:
+            self.err.zero_()
+            raise RuntimeError(
+                f"device error word 0x{e:x}: a plasma particle stencil left the grid "
+                "(NaN or runaway particle)" if e & _lib.DEVERR_PLASMA_STENCIL else
+                f"device error word 0x{e:x}")

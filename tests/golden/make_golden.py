@@ -15,6 +15,9 @@ Fixtures:
   run_rigid_bg.npz     -- full xi loop, rigid driver, background ions
   run_rigid_mobile.npz -- full xi loop, rigid driver, mobile ions
   run_beam.npz         -- full xi loop, generated (non-rigid) beam, 1 time step
+  run_test1.npz        -- the reference's own 3D golden configuration
+                          (tests/integration/test_3D_part.py:9-56): strided
+                          final state and on-axis Ez per xi step
 """
 import os
 import sys
@@ -228,7 +231,30 @@ def main(ref_root):
                    'default': {'length': 2.0}})
     np.savez_compressed(os.path.join(HERE, 'run_beam.npz'), **out)
     print('whole runs', time.time() - t, 's')
+    if '--test1' in sys.argv:
+        make_test1(lcode)
+
+
+def make_test1(lcode):
+    cfg = {'geometry': '3d', 'processing-unit-type': 'cpu',
+           'window-width': 8, 'transverse-step': 0.05,
+           'window-length': 10, 'xi-step': 0.05,
+           'time-limit': 1, 'time-step': 1, 'ion-model': 'background',
+           'plasma-particles-per-cell': 4,
+           'field-solver-subtraction-coefficient': 1.0}
+    out = run_sim(lcode, cfg, {'current': 0.05, 'particles_in_layer': 5000,
+                               'default': {'length': 5.013256548}})
+    keep = {'ez_axis': out['ez_axis'], 'ro_axis': out['ro_axis']}
+    for k, v in out.items():
+        if k.startswith('f_'):
+            keep[k] = v[::10, ::10]
+        elif k.startswith('c_'):
+            keep[k] = v[:, ::10, ::10].sum(axis=0)
+        elif k.startswith('p_electrons_'):
+            keep[k] = v[::10, ::10]
+    np.savez_compressed(os.path.join(HERE, 'run_test1.npz'), **keep)
 
 
 if __name__ == '__main__':
-    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+    args = [a for a in sys.argv[1:] if not a.startswith('--')]
+    main(args[0] if args else '/root/reference')

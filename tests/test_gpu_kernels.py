@@ -1,0 +1,309 @@
+"""Per-kernel parity of liblcb.so (called through its C ABI) against the CPU
+oracle and the reference's own known answers (tests/golden/kat_*.npz).
+
+Tolerances: the kernels compute in FP64 like the reference; the GPU sums in
+a different order (atomics, fused multiply-adds, dense transforms instead of
+FFTs), so results agree to a few ulps of the largest element."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover - CPU containers
+    pytest.skip("needs CUDA", allow_module_level=True)
+
+from lcodepy_b200 import _lib  # noqa: E402
+from lcodepy_b200.plasma3d import FieldOperators  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+DEV = torch.device("cuda")
+
+
+def T(a, dtype=torch.float64):
+    return torch.tensor(np.ascontiguousarray(a), dtype=dtype, device=DEV)
+
+
+def N_(t):
+    return t.detach().cpu().numpy()
+
+
+def close(got, ref, rel=1e-12, what=""):
+    scale = max(np.abs(ref).max(), 1e-300)
+    err = np.abs(got - ref).max() / scale
+    assert err <= rel, f"{what}: max |diff| / max |ref| = {err:.3e} > {rel:.1e}"
+
+
+@pytest.fixture(scope="module")
+def kat(golden):
+    return golden("kat_kernels.npz")
+
+
+def _plasma_from_kat(d):
+    n = d["x_init"].size
+    st = {k: T(d[v].ravel()) for k, v in (
+        ("x_init", "x_init"), ("y_init", "y_init"), ("x_offt", "xo_prev"),
+        ("y_offt", "yo_prev"), ("px", "px_prev"), ("py", "py_prev"),
+        ("pz", "pz_prev"), ("q", "q"), ("m", "m"))}
+    return n, st
+
+
+def test_move_wo_fields_and_smart(kat):
+    d = kat
+    L = _lib.load()
+    N, h, dxi, bnd = int(d["N"]), float(d["h"]), float(d["dxi"]), float(d["boundary"])
+    n, p = _plasma_from_kat(d)
+    full = {k: torch.empty_like(p["x_offt"]) for k in ("x_offt", "y_offt", "px", "py", "pz", "q")}
+    st = _lib.stream_handle()
+    _lib.check(L.lcb_plasma_move_wo_fields(
+        n, dxi, p["m"].data_ptr(), p["x_offt"].data_ptr(), p["y_offt"].data_ptr(),
+        p["px"].data_ptr(), p["py"].data_ptr(), p["pz"].data_ptr(), p["q"].data_ptr(),
+        full["x_offt"].data_ptr(), full["y_offt"].data_ptr(), full["px"].data_ptr(),
+        full["py"].data_ptr(), full["pz"].data_ptr(), full["q"].data_ptr(), st), "k1")
+    close(N_(full["x_offt"]).reshape(d["k1_xo"].shape), d["k1_xo"], 1e-15, "K1 x_offt")
+    close(N_(full["y_offt"]).reshape(d["k1_yo"].shape), d["k1_yo"], 1e-15, "K1 y_offt")
+    F = [T(d["F_" + k]) for k in ("Ex", "Ey", "Ez", "Bx", "By", "Bz")]
+    err = torch.zeros(1, dtype=torch.int32, device=DEV)
+    _lib.check(L.lcb_plasma_move_smart(
+        n, dxi, bnd, h, N, *(f.data_ptr() for f in F),
+        p["x_init"].data_ptr(), p["y_init"].data_ptr(), p["x_offt"].data_ptr(),
+        p["y_offt"].data_ptr(), p["px"].data_ptr(), p["py"].data_ptr(), p["pz"].data_ptr(),
+        p["m"].data_ptr(), full["q"].data_ptr(), full["x_offt"].data_ptr(),
+        full["y_offt"].data_ptr(), full["px"].data_ptr(), full["py"].data_ptr(),
+        full["pz"].data_ptr(), err.data_ptr(), st), "k2")
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    for k, ref in (("x_offt", "k2_xo"), ("y_offt", "k2_yo"), ("px", "k2_px"),
+                   ("py", "k2_py"), ("pz", "k2_pz"), ("q", "k2_q")):
+        close(N_(full[k]).reshape(d[ref].shape), d[ref], 1e-12, "K2 " + k)
+
+
+@pytest.mark.parametrize("precision,rel", [(_lib.LCB_PREC_FP64, 1e-12),
+                                           (_lib.LCB_PREC_MIXED, 2e-6)])
+def test_deposit(kat, precision, rel):
+    d = kat
+    L = _lib.load()
+    N, h = int(d["N"]), float(d["h"])
+    Ns = d["x_init"].shape[0]
+    n = Ns * Ns
+    x_init, y_init = T(d["x_init"].ravel()), T(d["y_init"].ravel())
+    xo, yo = T(d["k2_xo"].ravel()), T(d["k2_yo"].ravel())
+    px, py, pz = T(d["k2_px"].ravel()), T(d["k2_py"].ravel()), T(d["k2_pz"].ravel())
+    q, m = T(d["k2_q"].ravel()), T(d["m"].ravel())
+    out = [torch.full((2, N, N), 7.0, dtype=torch.float64, device=DEV) for _ in range(4)]
+    ro_init = T(np.arange(N * N, dtype=np.float64).reshape(N, N))
+    ws = torch.empty(max(L.lcb_plasma_deposit_workspace_bytes(N, precision), 256),
+                     dtype=torch.uint8, device=DEV)
+    err = torch.zeros(1, dtype=torch.int32, device=DEV)
+    _lib.check(L.lcb_plasma_deposit(
+        n, 1, N, h, Ns, precision, x_init.data_ptr(), y_init.data_ptr(), xo.data_ptr(),
+        yo.data_ptr(), px.data_ptr(), py.data_ptr(), pz.data_ptr(), q.data_ptr(),
+        m.data_ptr(), ro_init.data_ptr(), *(o.data_ptr() for o in out),
+        ws.data_ptr(), ws.numel(), err.data_ptr(), _lib.stream_handle()), "k3")
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    for o, k in zip(out, ("ro", "jx", "jy", "jz")):
+        close(N_(o[0]), d["k3_" + k], rel, "K3 " + k)
+    np.testing.assert_array_equal(N_(out[0][1]), N_(ro_init))
+    for o in out[1:]:
+        assert float(o[1].abs().max()) == 0.0
+
+
+def test_deposit_runaway_particles_take_global_path(kat):
+    """Particles far from their tile's window still deposit (global atomics)."""
+    d = kat
+    L = _lib.load()
+    N, h = int(d["N"]), float(d["h"])
+    Ns = d["x_init"].shape[0]
+    p = O.Params(N=N, h=h, dxi=float(d["dxi"]), sub_coeff=1, boundary=float(d["boundary"]))
+    rng = np.random.default_rng(3)
+    xo = rng.uniform(-0.8, 0.8, (Ns, Ns))  # up to 16 cells away from the lattice
+    yo = rng.uniform(-0.8, 0.8, (Ns, Ns))
+    xo = np.clip(d["x_init"] + xo, -1.0, 1.0) - d["x_init"]
+    yo = np.clip(d["y_init"] + yo, -1.0, 1.0) - d["y_init"]
+    s = O.Sort(d["x_init"], d["y_init"], xo, yo, d["k2_px"], d["k2_py"], d["k2_pz"],
+               d["k2_q"].copy(), d["m"])
+    cur = O.Currents.zeros(N)
+    O.deposit_sort(p, s, cur, 0)
+    out = [torch.zeros((2, N, N), dtype=torch.float64, device=DEV) for _ in range(4)]
+    ws = torch.empty(256, dtype=torch.uint8, device=DEV)
+    err = torch.zeros(1, dtype=torch.int32, device=DEV)
+    _lib.check(L.lcb_plasma_deposit(
+        Ns * Ns, 1, N, h, Ns, _lib.LCB_PREC_FP64, *(T(a.ravel()).data_ptr() for a in (
+            d["x_init"], d["y_init"], xo, yo, d["k2_px"], d["k2_py"], d["k2_pz"],
+            d["k2_q"], d["m"])), None, *(o.data_ptr() for o in out),
+        ws.data_ptr(), ws.numel(), err.data_ptr(), _lib.stream_handle()), "k3")
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    for o, k in zip(out, ("ro", "jx", "jy", "jz")):
+        close(N_(o[0]), getattr(cur, k)[0], 1e-12, "K3 " + k)
+
+
+def _fields_args(d, precision, ops, outs, ws):
+    N = int(d["N"])
+    keep = []
+
+    def t(a):
+        x = T(a)
+        keep.append(x)
+        return x.data_ptr()
+    a = _lib.ComputeFieldsArgs()
+    a.grid_steps, a.h, a.xi_step = N, float(d["h"]), float(d["dxi"])
+    a.subtraction_coeff, a.precision = float(d["sub"]), precision
+    a.consts = ops.struct
+    for i, k in enumerate(("Ex", "Ey", "Ez", "Bx", "By", "Bz", "Phi")):
+        a.fields.f[i] = t(d["in_" + k])
+        a.fields_prev.f[i] = t(d["prev_" + k])
+        a.out_full.f[i] = outs[0][i].data_ptr()
+        a.out_half.f[i] = outs[1][i].data_ptr()
+    a.currents_prev = _lib.Currents4(*(t(d["cp_" + k]) for k in ("ro", "jx", "jy", "jz")), 2)
+    a.currents_full = _lib.Currents4(*(t(d["cf_" + k]) for k in ("ro", "jx", "jy", "jz")), 2)
+    a.rho_beam_full, a.rho_beam_prev = t(d["rb_full"]), t(d["rb_prev"])
+    a.rho_beam_divisor = 1.0
+    a.workspace, a.workspace_bytes = ws.data_ptr(), ws.numel()
+    return a, keep
+
+
+@pytest.mark.parametrize("precision,rel", [(_lib.LCB_PREC_FP64, 1e-11),
+                                           (_lib.LCB_PREC_MIXED, 3e-5)])
+def test_compute_fields(golden, precision, rel):
+    d = golden("kat_fields.npz")
+    L = _lib.load()
+    N = int(d["N"])
+    ops = FieldOperators(N, float(d["h"]), float(d["sub"]), DEV,
+                         precision == _lib.LCB_PREC_MIXED)
+    outs = [torch.full((7, N, N), 3.0, dtype=torch.float64, device=DEV) for _ in range(2)]
+    ws = torch.empty(L.lcb_compute_fields_workspace_bytes(N, precision), dtype=torch.uint8,
+                     device=DEV)
+    a, keep = _fields_args(d, precision, ops, outs, ws)
+    _lib.check(L.lcb_compute_fields(C.byref(a), _lib.stream_handle()), "compute_fields")
+    torch.cuda.synchronize()
+    for i, k in enumerate(("Ex", "Ey", "Ez", "Bx", "By", "Bz", "Phi")):
+        close(N_(outs[0][i]), d["full_" + k], rel, "full " + k)
+        close(N_(outs[1][i]), d["half_" + k], rel, "half " + k)
+
+
+@pytest.mark.parametrize("N", [33, 129, 257])
+def test_compute_fields_sizes_vs_oracle(N):
+    """Random smooth currents at several grid sizes (both GEMM tilings)."""
+    L = _lib.load()
+    h, dxi = 0.05, 0.05
+    rng = np.random.default_rng(N)
+    p = O.Params(N=N, h=h, dxi=dxi, sub_coeff=1 + dxi, boundary=0)
+    consts = O.Consts(None, O.dirichlet_matrix(N, h), O.mixed_matrix(N, h, 1 + dxi),
+                      O.neumann_matrix(N, h))
+
+    def cur():
+        a = np.zeros((2, N, N))
+        a[:, 3:-3, 3:-3] = rng.normal(0, 1, (2, N - 6, N - 6))
+        return a
+    cp = O.Currents(cur(), cur(), cur(), cur())
+    cf = O.Currents(cur(), cur(), cur(), cur())
+    F = O.Fields(*(rng.normal(0, 1, (N, N)) for _ in range(7)))
+    Fp = O.Fields(*(rng.normal(0, 1, (N, N)) for _ in range(7)))
+    for f in (F, Fp):  # fields vanish on the walls, as the solver produces them
+        for k in ("Ex", "Ey", "Ez", "Bx", "By", "Phi"):
+            getattr(f, k)[[0, -1], :] = 0
+            getattr(f, k)[:, [0, -1]] = 0
+    rbf, rbp = rng.normal(0, 1, (N, N)), rng.normal(0, 1, (N, N))
+    full, half = O.compute_fields(p, F, Fp, consts, rbf, rbp, cp, cf)
+    d = {"N": N, "h": h, "dxi": dxi, "sub": 1 + dxi, "rb_full": rbf, "rb_prev": rbp}
+    for k in ("ro", "jx", "jy", "jz"):
+        d["cp_" + k], d["cf_" + k] = getattr(cp, k), getattr(cf, k)
+    for k in ("Ex", "Ey", "Ez", "Bx", "By", "Bz", "Phi"):
+        d["in_" + k], d["prev_" + k] = getattr(F, k), getattr(Fp, k)
+    ops = FieldOperators(N, h, 1 + dxi, DEV, False)
+    outs = [torch.zeros((7, N, N), dtype=torch.float64, device=DEV) for _ in range(2)]
+    ws = torch.empty(L.lcb_compute_fields_workspace_bytes(N, 0), dtype=torch.uint8, device=DEV)
+    a, keep = _fields_args(d, 0, ops, outs, ws)
+    _lib.check(L.lcb_compute_fields(C.byref(a), _lib.stream_handle()), "compute_fields")
+    torch.cuda.synchronize()
+    for i, k in enumerate(("Ex", "Ey", "Ez", "Bx", "By", "Bz", "Phi")):
+        close(N_(outs[0][i]), getattr(full, k), 1e-11, f"N={N} full {k}")
+        close(N_(outs[1][i]), getattr(half, k), 1e-11, f"N={N} half {k}")
+
+
+def test_beam_deposit_and_substepping(kat):
+    d = kat
+    L = _lib.load()
+    N, h, dxi = int(d["N"]), float(d["h"]), float(d["dxi"])
+    x, y, xi, q = (T(d[k]) for k in ("b_x", "b_y", "b_xi", "b_q"))
+    r0 = torch.zeros(N, N, dtype=torch.float64, device=DEV)
+    r1 = torch.zeros_like(r0)
+    err = torch.zeros(1, dtype=torch.int32, device=DEV)
+    _lib.check(L.lcb_beam_deposit(x.numel(), N, h, dxi, int(d["b_layer"]), x.data_ptr(),
+                                  y.data_ptr(), xi.data_ptr(), q.data_ptr(), r0.data_ptr(),
+                                  r1.data_ptr(), err.data_ptr(), _lib.stream_handle()), "k4")
+    qm, pz = T(d["k6_qm"]), T(d["k6_pz"])
+    dt = torch.zeros_like(qm)
+    rs = torch.zeros(qm.numel(), dtype=torch.int64, device=DEV)
+    _lib.check(L.lcb_beam_substepping(qm.numel(), qm.data_ptr(), pz.data_ptr(), 2.0, 1.0,
+                                      dt.data_ptr(), rs.data_ptr(), _lib.stream_handle()), "k6")
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    close(N_(r0), d["k4_ro0"], 1e-12, "K4 ro0")
+    close(N_(r1), d["k4_ro1"], 1e-12, "K4 ro1")
+    np.testing.assert_array_equal(N_(dt), d["k6_dt"])
+    np.testing.assert_array_equal(N_(rs), (1.0 / d["k6_dt"]).astype(np.int64))
+
+
+def test_beam_move_vs_oracle():
+    """Substepped Higuera-Cary push of a layer against the oracle restatement,
+    including particles that fall to the next layer and particles lost at the
+    wall."""
+    L = _lib.load()
+    N, h, dxi = 65, 0.05, 0.05
+    p = O.Params(N=N, h=h, dxi=dxi, sub_coeff=1, boundary=0)
+    rng = np.random.default_rng(11)
+    n = 3000
+    layer = 9
+    b = O.Beam(xi=rng.uniform(-(layer) * dxi, -(layer - 1) * dxi, n),
+               x=rng.normal(0, 0.5, n), y=rng.normal(0, 0.5, n),
+               px=rng.normal(0, 5, n), py=rng.normal(0, 5, n),
+               pz=rng.choice([-50.0, 0.3, 20.0, 1000.0], n),
+               q_m=rng.choice([-1.0, 1.0, 1 / 1836.0], n), q_norm=np.ones(n),
+               id=np.arange(1, n + 1, dtype=np.int64), dt=np.zeros(n),
+               remaining_steps=np.zeros(n, np.int64))
+    b.x[:20] = 1.4  # near / beyond the loss radius
+    X, Y = np.meshgrid(np.arange(N), np.arange(N), indexing="ij")
+    Fk = O.Fields(*(0.3 * np.sin(0.2 * (i + 1) * X + 0.1 * Y) for i in range(6)), np.zeros((N, N)))
+    Fk1 = O.Fields(*(0.3 * np.cos(0.15 * (i + 1) * Y - 0.1 * X) for i in range(6)), np.zeros((N, N)))
+    g = {k: T(getattr(b, k)) for k in ("xi", "x", "y", "px", "py", "pz", "q_m")}
+    g["id"] = T(b.id, torch.int64)
+    g["dt"] = torch.zeros(n, dtype=torch.float64, device=DEV)
+    g["rs"] = torch.zeros(n, dtype=torch.int64, device=DEV)
+    fell_size = 200
+    rs0 = rng.integers(1, 4, fell_size)
+    dt0 = 1.0 / rs0
+    b.remaining_steps[n - fell_size:] = rs0
+    b.dt[n - fell_size:] = dt0
+    g["rs"][n - fell_size:] = T(rs0, torch.int64)
+    g["dt"][n - fell_size:] = T(dt0)
+    lost, moved, fell = O.move_beam_layer(p, b, fell_size, layer, Fk, Fk1, 1.0, 2.0)
+    _lib.check(L.lcb_beam_substepping(n - fell_size, g["q_m"].data_ptr(), g["pz"].data_ptr(),
+                                      2.0, 1.0, g["dt"].data_ptr(), g["rs"].data_ptr(),
+                                      _lib.stream_handle()), "k6")
+    fk = [T(getattr(Fk, k)) for k in ("Ex", "Ey", "Ez", "Bx", "By", "Bz", "Phi")]
+    fk1 = [T(getattr(Fk1, k)) for k in ("Ex", "Ey", "Ez", "Bx", "By", "Bz", "Phi")]
+    s0, s1 = _lib.Fields7(), _lib.Fields7()
+    for i in range(7):
+        s0.f[i], s1.f[i] = fk[i].data_ptr(), fk1[i].data_ptr()
+    flags = torch.zeros(n, dtype=torch.uint8, device=DEV)
+    err = torch.zeros(1, dtype=torch.int32, device=DEV)
+    R = h * N / 2
+    _lib.check(L.lcb_beam_move(n, dxi, max(0.9 * R, R - 1), layer - 1, h, N,
+                               g["q_m"].data_ptr(), g["dt"].data_ptr(), s0, s1,
+                               g["rs"].data_ptr(), g["id"].data_ptr(), g["x"].data_ptr(),
+                               g["y"].data_ptr(), g["xi"].data_ptr(), g["px"].data_ptr(),
+                               g["py"].data_ptr(), g["pz"].data_ptr(), flags.data_ptr(),
+                               err.data_ptr(), _lib.stream_handle()), "k5")
+    torch.cuda.synchronize()
+    fl = N_(flags)
+    for sel, ref in ((fl & 1, lost), (fl & 2, moved), (fl & 4, fell)):
+        idx = np.nonzero(sel)[0]
+        np.testing.assert_array_equal(N_(g["id"])[idx], ref.id)
+        for k in ("x", "y", "xi", "px", "py", "pz"):
+            close(N_(g[k])[idx], getattr(ref, k), 1e-11, k)
+    assert lost.size > 0 and moved.size > 0 and fell.size > 0

@@ -1,0 +1,146 @@
+"""Whole xi loops through the drop-in ``Simulation`` on the GPU, against runs
+of the reference (tests/golden/run_*.npz, made by make_golden.py) and the
+CPU oracle."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("needs CUDA", allow_module_level=True)
+
+from lcodepy_b200 import Simulation  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+
+def rigid_driver(xp, xi, x, y):
+    if -np.sqrt(2 * np.pi) <= xi <= 0:
+        return 0.1 * xp.exp(-(x ** 2 + y ** 2) / 2) * (1 + np.cos(np.sqrt(np.pi / 2) * xi)) / 2
+    return xp.zeros_like(x)
+
+
+def cfg(**kw):
+    c = {'geometry': '3d', 'processing-unit-type': 'gpu',
+         'window-width': 1.6, 'transverse-step': 0.05,
+         'window-length': 2.0, 'xi-step': 0.05,
+         'time-limit': 1, 'time-step': 1,
+         'ion-model': 'background', 'plasma-particles-per-cell': 4,
+         'print-every': 0}
+    c.update(kw)
+    return c
+
+
+def run(config, beam, n_steps=None):
+    sim = Simulation(config=config, beam_parameters=beam, diagnostics=[], runas_filename='')
+    sim.step(n_steps)
+    ps = sim.push_solver
+    particles, fields, currents = ps._plasmastate
+    return sim, particles, fields, currents, ps.ez_axis.cpu().numpy()
+
+
+def rel_err(got, ref):
+    return np.abs(got - ref).max() / max(np.abs(ref).max(), 1e-300)
+
+
+def check(ref, particles, fields, currents, sorts, rel):
+    for k in ("Ex", "Ey", "Ez", "Bx", "By", "Bz", "Phi"):
+        e = rel_err(getattr(fields, k).cpu().numpy(), ref["f_" + k])
+        assert e < rel, f"{k}: {e:.2e}"
+    for k in ("ro", "jx", "jy", "jz"):
+        e = rel_err(getattr(currents, k).cpu().numpy(), ref["c_" + k])
+        assert e < rel, f"{k}: {e:.2e}"
+    for s in sorts:
+        for k in ("x_offt", "y_offt", "px", "py", "pz", "q"):
+            e = rel_err(getattr(particles[s], k).cpu().numpy(), ref[f"p_{s}_{k}"])
+            assert e < rel, f"{s}.{k}: {e:.2e}"
+
+
+@pytest.mark.parametrize("fixture,extra,sorts", [
+    ("run_rigid_bg.npz", {}, ["electrons"]),
+    ("run_rigid_mobile.npz", {'ion-model': 'mobile', 'window-length': 1.0, 'xi-step': 0.1},
+     ["electrons", "ions"]),
+])
+def test_rigid_vs_reference(golden, fixture, extra, sorts):
+    ref = golden(fixture)
+    _, particles, fields, currents, ez = run(cfg(**{'rigid-beam': True, **extra}), rigid_driver)
+    assert rel_err(ez, ref["ez_axis"]) < 1e-9
+    check(ref, particles, fields, currents, sorts, 1e-8)
+
+
+def test_generated_beam_vs_reference(golden):
+    ref = golden("run_beam.npz")
+    _, particles, fields, currents, ez = run(
+        cfg(**{'window-length': 1.5}),
+        {'current': 0.05, 'particles_in_layer': 400, 'default': {'length': 2.0}})
+    assert rel_err(ez, ref["ez_axis"]) < 1e-9
+    check(ref, particles, fields, currents, ["electrons"], 1e-8)
+
+
+def test_reference_golden_configuration(golden):
+    """The reference's own 3D golden case (N=321, 201 xi steps, generated beam),
+    checked exactly as the reference's test checks it (rtol 5e-8)."""
+    ref = golden("run_test1.npz")
+    c = {'geometry': '3d', 'processing-unit-type': 'gpu', 'window-width': 8,
+         'transverse-step': 0.05, 'window-length': 10, 'xi-step': 0.05,
+         'time-limit': 1, 'time-step': 1, 'ion-model': 'background',
+         'plasma-particles-per-cell': 4, 'field-solver-subtraction-coefficient': 1.0,
+         'print-every': 0}
+    _, particles, fields, currents, ez = run(
+        c, {'current': 0.05, 'particles_in_layer': 5000, 'default': {'length': 5.013256548}})
+    el = particles["electrons"]
+    for a in ("x_offt", "y_offt", "px", "py", "pz"):
+        np.testing.assert_allclose(getattr(el, a).cpu().numpy()[::10, ::10],
+                                   ref["p_electrons_" + a], rtol=5e-8,
+                                   atol=1e-8 * np.abs(ref["p_electrons_" + a]).max())
+    for a in ("Ex", "Ey", "Ez", "Bx", "By", "Bz"):
+        np.testing.assert_allclose(getattr(fields, a).cpu().numpy()[::10, ::10],
+                                   ref["f_" + a], rtol=5e-8, atol=1e-8 * np.abs(ref["f_" + a]).max())
+    for a in ("ro", "jx", "jy", "jz"):
+        np.testing.assert_allclose(getattr(currents, a).cpu().numpy()[:, ::10, ::10].sum(axis=0),
+                                   ref["c_" + a], rtol=5e-8, atol=1e-8 * np.abs(ref["c_" + a]).max())
+    assert rel_err(ez, ref["ez_axis"]) < 5e-8
+
+
+def test_two_time_steps_beam_push_vs_oracle():
+    """Second time step depends on the beam push (GPU Higuera-Cary algorithm),
+    checked against the oracle's restatement of it."""
+    from lcodepy_b200.beam_generator import generate_beam
+    from lcodepy_b200.config import Config
+    config = cfg(**{'window-length': 1.5, 'time-limit': 2, 'time-step': 5.0})
+    beam_params = {'current': -0.5, 'particles_in_layer': 300,
+                   'default': {'length': 1.2, 'energy': 5.0, 'angspread': 1e-2}}
+    sim, particles, fields, currents, ez = run(config, beam_params, n_steps=2)
+    c = Config(config)
+    c._adjust_config_values_3d()
+    beam = O.Beam.from_array(generate_beam(c, beam_params)).sorted()
+    p = O.make_params(1.6, 0.05, 0.05)
+    xi_steps = round(1.5 / 0.05)
+    for t in range(2):
+        sorts, consts = O.init_plasma(p)
+        F, cur = O.Fields.zeros(p.N), O.Currents.zeros(p.N)
+        ez_o = []
+        rec = lambda i, s, f, cc, rb: ez_o.append(f.Ez[p.N // 2, p.N // 2])
+        sorts, F, cur, drain = O.step_dt(p, sorts, F, cur, consts, xi_steps, beam=beam,
+                                         time_step=5.0, record=rec)
+        beam = drain.sorted()
+    assert rel_err(ez, np.array(ez_o)) < 1e-8
+    assert rel_err(fields.Ez.cpu().numpy(), F.Ez) < 1e-8
+    got = sim.beam_drain.beam_slice()
+    order = np.argsort(got.id.cpu().numpy())
+    ref_order = np.argsort(drain.id)
+    np.testing.assert_array_equal(got.id.cpu().numpy()[order], drain.id[ref_order])
+    for k in ("x", "y", "xi", "px", "py", "pz"):
+        assert rel_err(getattr(got, k).cpu().numpy()[order], getattr(drain, k)[ref_order]) < 1e-9, k
+
+
+def test_mixed_precision_on_axis_ez():
+    """FP32 deposition and FP32 transforms, FP64 particles: on-axis Ez within
+    relative L2 1e-5 of the FP64 run (rigid driver, 129 x 129, 201 xi steps)."""
+    base = cfg(**{'rigid-beam': True, 'window-width': 6.5, 'transverse-step': 0.1,
+                  'xi-step': 0.1, 'window-length': 20})
+    _, _, f64, _, ez64 = run(base, rigid_driver)
+    _, _, fmx, _, ezmx = run({**base, 'precision': 'mixed'}, rigid_driver)
+    l2 = np.linalg.norm(ezmx - ez64) / np.linalg.norm(ez64)
+    print("mixed vs fp64 on-axis Ez rel L2:", l2)
+    assert l2 < 1e-5
