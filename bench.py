@@ -1,0 +1,374 @@
+#!/usr/bin/env python
+"""Benchmark: xi-steps x cells per second of the quasistatic 3D xi loop.
+
+Workload (the production FP64 drop-in configuration): 513 x 513 grid
+(window-width 5.13, transverse-step 0.02), 2 x 2 plasma macroparticles per
+cell (929,296 electrons, background ions), xi-step 0.02, window-length 60
+(3001 xi iterations), and a non-rigid seeded bi-Gaussian electron driver of
+1,000,000 macroparticles (sigma_r 0.5, sigma_z 1, peak n_b/n0 = 0.5,
+gamma = 1000 +- 1 %, normalised emittance 1e-2), pushed every xi layer.
+
+One bench step = one xi step (plasma predictor-corrector + beam layout and
+push) of that workload; the xi loop of one time step runs once, the first
+--warmup xi steps untimed and the next --steps timed with CUDA events.  All
+inputs live in HBM and exceed L2 (plasma state 134 MB, beam 88 MB), so no
+extra L2 flush is done.  With --gpus N (torchrun) every rank runs its own
+replica (the xi loop does not shard): weak scaling.
+
+--impl reference times the CPU restatement of the reference algorithm
+(oracle/, the reference's own numba path cannot be shipped here) on the
+host cores, on a bounded prefix of the same xi loop.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "lcode3d-production-fp64: N=513 h=0.02 ppc=4 dxi=0.02 L=60 beam=1e6 bi-gaussian"
+METRIC = "xi-steps*cells/s"
+
+
+def workload_config(precision="fp64"):
+    return {'geometry': '3d', 'processing-unit-type': 'gpu',
+            'window-width': 5.13, 'transverse-step': 0.02,
+            'window-length': 60.0, 'xi-step': 0.02,
+            'time-limit': 1.0, 'time-step': 1.0,
+            'ion-model': 'background', 'plasma-particles-per-cell': 4,
+            'rigid-beam': False, 'print-every': 0, 'precision': precision}
+
+
+def make_beam(n=1_000_000, seed=2024, sigma_r=0.5, sigma_z=1.0, xi0=-3.0,
+              gamma=1000.0, espread=0.01, emittance=1e-2, peak=-0.5, dxi=0.02,
+              r_max=4.0):
+    """Seeded bi-Gaussian driver as a particle_dtype3d array.  q_norm makes the
+    deposited on-axis peak density equal `peak` (layer charge per cell area):
+    rho = Q dxi / (sqrt(2 pi) sigma_z) / (2 pi sigma_r^2)."""
+    from lcodepy_b200.beam_generator import particle_dtype3d
+    rng = np.random.default_rng(seed)
+    xi = rng.normal(xi0, sigma_z, 2 * n)
+    xi = xi[(xi < 0) & (xi > 2 * xi0)][:n]
+    m = xi.size
+    r = sigma_r * np.sqrt(-2 * np.log(1 - rng.random(m) * (1 - np.exp(-r_max ** 2 / (2 * sigma_r ** 2)))))
+    phi = rng.uniform(0, 2 * np.pi, m)
+    b = np.zeros(m, dtype=particle_dtype3d)
+    b['xi'] = xi
+    b['x'], b['y'] = r * np.cos(phi), r * np.sin(phi)
+    sp = emittance / sigma_r
+    b['px'], b['py'] = rng.normal(0, sp, m), rng.normal(0, sp, m)
+    b['pz'] = rng.normal(gamma, gamma * espread, m)
+    b['q_m'] = -1.0
+    q_total = peak * (np.sqrt(2 * np.pi) * sigma_z) * (2 * np.pi * sigma_r ** 2) / dxi
+    b['q_norm'] = q_total / m
+    b['id'] = np.arange(1, m + 1)
+    return b[np.argsort(-b['xi'])]
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--id={index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [ln.split(",") for ln in open(self.f.name).read().splitlines() if ln.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init():
+    import torch
+    import torch.distributed as dist
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def max_over_ranks(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64,
+                     device="cuda" if torch.cuda.is_available() else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+def run_gpu(args, ws, rank, local):
+    import torch
+    from lcodepy_b200 import Simulation, _lib
+    from lcodepy_b200.beam3d import BeamParticles, BeamSource, BeamDrain
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    cfg = workload_config(args.precision)
+    beam_host = make_beam()
+    sim = Simulation(config=cfg, beam_parameters={}, runas_filename='')
+    ps = sim.push_solver
+    conf = sim.effective_config
+    N = conf.getint('window-width-steps')
+    n_iter = ps.xi_steps + 1
+    W, K = args.warmup, args.steps
+    if W + K > n_iter:
+        raise SystemExit(f"--warmup + --steps must be <= {n_iter} xi steps")
+
+    # ---- device-resident timed run: one xi loop, events at W and W+K ----
+    source = BeamSource(conf, BeamParticles(dev).init_generated(beam_host), dev)
+    drain = BeamDrain(conf, dev)
+    ps.plasma_solver.init_state(1.0)
+    torch.cuda.synchronize()
+    ev = {}
+    op_times = {}
+
+    def hook(k):
+        if k == W:
+            barrier(ws)
+            torch.cuda.synchronize()
+            ev["clock"] = ClockSampler(local) if rank == 0 else None
+            ev["l0"] = _lib.launch_count()
+            ev["t0"] = torch.cuda.Event(enable_timing=True)
+            ev["t0"].record()
+            ps.plasma_solver.op_timers = op_times
+        if k == W + K:
+            ev["t1"] = torch.cuda.Event(enable_timing=True)
+            ev["t1"].record()
+            ps.plasma_solver.op_timers = None
+            torch.cuda.synchronize()
+            ev["l1"] = _lib.launch_count()
+            ev["clocks"] = ev["clock"].stop() if ev.get("clock") else None
+
+    ps.step_dt(conf.getfloat('xi-step'), source, drain, 1.0, [], step_hook=hook)
+    if "t1" not in ev:
+        hook(W + K)
+    torch.cuda.synchronize()
+    ms_total = ev["t0"].elapsed_time(ev["t1"])
+    ms_total = max_over_ranks(ms_total, ws)
+    barrier(ws)
+    ms_per_step = ms_total / K
+    cells = N * N
+    value = ws * K * cells / (ms_total / 1e3)
+
+    # ---- per-op device time over the timed region (CUDA events) ----
+    ops = {}
+    for name, evs in op_times.items():
+        tot = sum(a.elapsed_time(b) for a, b in evs)
+        ops[name] = {"launches": len(evs), "ms_total": tot, "ms_avg": tot / max(len(evs), 1)}
+
+    # ---- end to end through the public API, host buffers in and out ----
+    e2e = run_e2e(cfg, beam_host, dev)
+
+    return dict(value=value, ms_per_step=ms_per_step, N=N, ops=ops,
+                launches=int(ev["l1"] - ev["l0"]), clocks=ev.get("clocks"),
+                e2e=e2e, n_iter=n_iter)
+
+
+def run_e2e(cfg, beam_host, dev):
+    """Simulation.step() from a host beam file to host results: the H2D copy of
+    the beam and of the initial plasma and the D2H read of fields, on-axis Ez
+    and the moved beam are inside the timed region."""
+    import torch
+    from lcodepy_b200 import Simulation
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "beam.npz")
+        np.savez(path, **{k: beam_host[k] for k in beam_host.dtype.names})
+        sim = Simulation(config=cfg, beam_parameters={}, runas_filename='')
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sim.load_beamfile(path)
+        sim.step(1)
+        particles, fields, currents = sim.push_solver._plasmastate
+        host_fields = fields.to_numpy()
+        ez = sim.push_solver.ez_axis.cpu().numpy()
+        moved = sim.beam_drain.beam_slice().particles
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+    conf = sim.effective_config
+    N = conf.getint('window-width-steps')
+    n_iter = sim.push_solver.xi_steps + 1
+    Ns = sim.push_solver.plasma_solver.states[0].Ns
+    h2d = beam_host.nbytes + 4 * Ns * Ns * 8
+    d2h = 7 * N * N * 8 + ez.nbytes + moved.nbytes
+    return {"value": n_iter * N * N / dt, "unit": METRIC, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "seconds": dt, "xi_steps": n_iter}
+
+
+# ---------------------------------------------------------------------------
+# CPU arm (oracle restatement of the reference algorithm)
+# ---------------------------------------------------------------------------
+
+def run_cpu_sample(xi_steps_sample, beam_host):
+    """The oracle on the host cores for the first `xi_steps_sample` xi steps of
+    the workload; returns (xi-steps*cells/s, seconds, threads)."""
+    from oracle import oracle as O
+    p = O.make_params(5.13, 0.02, 0.02)
+    sorts, consts = O.init_plasma(p)
+    F, cur = O.Fields.zeros(p.N), O.Currents.zeros(p.N)
+    beam = O.Beam.from_array(beam_host).sorted()
+    t0 = time.perf_counter()
+    O.step_dt(p, sorts, F, cur, consts, xi_steps_sample - 1, beam=beam, time_step=1.0)
+    dt = time.perf_counter() - t0
+    return xi_steps_sample * p.N * p.N / dt, dt, O.num_threads()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2997)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--cpu-sample", type=int, default=8,
+                    help="xi steps of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be >= 3")
+    ws, rank, local = dist_init()
+
+    if args.impl == "reference":
+        if rank == 0:
+            beam = make_beam()
+            n = max(2, min(args.steps, args.cpu_sample))
+            v, dt, thr = run_cpu_sample(n, beam)
+            line = {"metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
+                    "steps": n, "warmup": 0, "ms_per_step": dt * 1e3 / n,
+                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                    "dtype": "f64", "data": "synthetic", "impl": "reference",
+                    "config": {"workload": WORKLOAD, "parallelism": "replicas",
+                               "l2": "inputs larger than L2"},
+                    "cpu_baseline": {"value": v, "unit": METRIC, "cores": thr, "kind": "port",
+                                     "sample": f"first {n} xi steps of the workload "
+                                               "(oracle/: C particle loops + scipy DST/DCT)"},
+                    "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0,
+                            "d2h_bytes_per_step": 0}}
+            print(json.dumps(line), flush=True)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    r = run_gpu(args, ws, rank, local)
+    if rank == 0:
+        N = r["N"]
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except (OSError, ValueError):
+            pass
+        hbm_peak = peaks.get("hbm_gbs", 6650.0)
+        peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+        r["precision"] = args.precision
+        roof = roofline(r, N, hbm_peak, peak_src, peaks)
+        cpu = None
+        if not args.no_cpu_baseline:
+            v, dt, thr = run_cpu_sample(args.cpu_sample, make_beam())
+            cpu = {"value": v, "unit": METRIC, "cores": thr, "kind": "port",
+                   "sample": f"first {args.cpu_sample} xi steps of the workload on the host "
+                             f"({dt:.1f} s; oracle/: C particle loops, scipy DST/DCT)"}
+        line = {"metric": METRIC, "value": r["value"], "unit": METRIC, "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "f64-particles/f32-fields",
+                "data": "synthetic (seeded bi-Gaussian beam, uniform plasma)",
+                "config": {"workload": WORKLOAD, "grid": N, "xi_iterations": r["n_iter"],
+                           "precision": args.precision, "parallelism": "replicas",
+                           "l2": "inputs larger than L2 (no flush)"},
+                "e2e": {k: r["e2e"][k] for k in ("value", "unit", "h2d_bytes_per_step",
+                                                 "d2h_bytes_per_step")},
+                "gpu_launches": r["launches"], "clocks": r["clocks"],
+                "roofline": roof, "cpu_baseline": cpu,
+                "ops": {k: {"launches": v["launches"], "ms_avg": round(v["ms_avg"], 5),
+                            "ms_total": round(v["ms_total"], 2)} for k, v in r["ops"].items()}}
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def roofline(r, N, hbm_peak, peak_src, peaks):
+    """Roofline of the dominant operation over the timed region."""
+    ops = r["ops"]
+    if not ops:
+        return None
+    name = max(ops, key=lambda k: ops[k]["ms_total"])
+    o = ops[name]
+    Np = 964 * 964
+    if name == "compute_fields":
+        # 4 waves x 7 problems, each 2*M*N*K; roughly 56 N^3 flops per call
+        flops = 56.0 * N ** 3
+        achieved = flops / (o["ms_avg"] / 1e3) / 1e12
+        peak = 37.0 if r.get("precision", "fp64") == "fp64" else peaks.get("bf16_tflops", 1590.0)
+        return {"bound": "fp64-simt", "kernel": name, "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                "peak_source": "nominal B200 FP64 (no measured FP64 peak)"}
+    per = {"deposit": 72, "move_smart": 128, "move_wo_fields": 64}.get(name, 0)
+    achieved = per * Np / (o["ms_avg"] / 1e3) / 1e9
+    return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm_peak,
+            "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+            "peak_source": peak_src}
+
+
+if __name__ == "__main__":
+    main()

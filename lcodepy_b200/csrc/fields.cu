@@ -273,6 +273,7 @@ struct FinishArgs {
     const double *bz_raw, *bz_sum, *bz_prev;
     double *bz_full, *bz_half;
     double *half[7], *full[7];
+    const double *prev[7];
 };
 
 __global__ void __launch_bounds__(256) k_fields_finish(FinishArgs a)
@@ -287,14 +288,18 @@ __global__ void __launch_bounds__(256) k_fields_finish(FinishArgs a)
         if (a.bz_half) a.bz_half[t] = (v + a.bz_prev[t]) / 2;
         const int i = (int)(t / N), j = (int)(t % N);
         const bool row_edge = (i == 0 || i == N - 1), col_edge = (j == 0 || j == N - 1);
-        // Ex(0), By(4): zero columns; Ey(1), Bx(3): zero rows; Ez(2), Phi(6): both.
-        const bool zero[7] = {col_edge, row_edge, row_edge || col_edge, row_edge,
+        // The solutions are zero on their Dirichlet edges: Ex(0), By(4) on the
+        // first/last column, Ey(1), Bx(3) on the first/last row, Ez(2), Phi(6)
+        // on all four.  There the reference's combinations reduce to
+        // full = 2*0 - prev (transverse), Ez half = (0 + prev)/2, Phi = 0.
+        const bool edge[7] = {col_edge, row_edge, row_edge || col_edge, row_edge,
                               col_edge, false, row_edge || col_edge};
 #pragma unroll
         for (int f = 0; f < 7; f++) {
-            if (!zero[f]) continue;
-            if (a.half[f]) a.half[f][t] = 0.0;
-            if (a.full[f]) a.full[f][t] = 0.0;
+            if (!edge[f] || f == 5) continue;
+            const bool transverse = (f == 0 || f == 1 || f == 3 || f == 4);
+            if (a.half[f]) a.half[f][t] = (f == 2) ? (0.0 + a.prev[f][t]) / 2 : 0.0;
+            if (a.full[f]) a.full[f][t] = transverse ? 2 * 0.0 - a.prev[f][t] : 0.0;
         }
     }
 }
@@ -462,7 +467,11 @@ static int solve(const lcb_compute_fields_args *a, const Ops<T> &op, cudaStream_
     fa.N = N; fa.bz_raw = w.bz_raw; fa.bz_sum = w.bz_sum;
     fa.bz_prev = a->fields_prev.f[5];
     fa.bz_full = a->out_full.f[5]; fa.bz_half = a->out_half.f[5];
-    for (int f = 0; f < 7; f++) { fa.half[f] = a->out_half.f[f]; fa.full[f] = a->out_full.f[f]; }
+    for (int f = 0; f < 7; f++) {
+        fa.half[f] = a->out_half.f[f];
+        fa.full[f] = a->out_full.f[f];
+        fa.prev[f] = a->fields_prev.f[f];
+    }
     {
         const int64_t tot = (int64_t)N * N;
         int blocks = (int)((tot + 255) / 256);

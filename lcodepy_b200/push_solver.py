@@ -41,9 +41,11 @@ class PusherAndSolver3D:
         self.lost = []
 
     def step_dt(self, xi_plasma_layer_start, beam_source, beam_drain,
-                current_time, diagnostics_list=()):
+                current_time, diagnostics_list=(), step_hook=None):
         """Run the xi loop of one time step.  The plasma state must have been
-        initialised on the solver (Simulation does this)."""
+        initialised on the solver (Simulation does this).  ``step_hook(k)``,
+        if given, is called before the k-th xi step and once after the last
+        (k = number of steps); the benchmark uses it to place its events."""
         ps = self.plasma_solver
         bc = self.beam_calculator
         N = self.grid_steps
@@ -59,6 +61,8 @@ class PusherAndSolver3D:
         fell_size = 0
         self.lost = []
         for k, xi_i in enumerate(range(first, last + 1)):
+            if step_hook is not None:
+                step_hook(k)
             if self.rigid:
                 rb_full, rb_prev = bc.layout_beam_layer(None, xi_i)
                 layer = None
@@ -84,6 +88,8 @@ class PusherAndSolver3D:
                                      ps.prev_fields.arrays().wrapped(),
                                      ps.prev_currents.arrays().wrapped(),
                                      Arrays(None, r=rho).wrapped().r)
+        if step_hook is not None:
+            step_hook(n_iter)
         ps.check_errors()
         if not self.rigid:
             e = int(bc.err.item())

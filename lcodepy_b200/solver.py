@@ -90,6 +90,19 @@ class Plane2d3vPlasmaSolver:
         self.zero_plane = torch.zeros(N, N, dtype=torch.float64, device=dev)
         self.states = None
         self.cur = 0  # index of the "prev" copy in self.states / fields / currents
+        # name -> list of (start, end) CUDA events, filled while not None
+        self.op_timers = None
+
+    def _timed(self, name, fn, *args):
+        if self.op_timers is None:
+            return fn(*args)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        r = fn(*args)
+        b.record()
+        self.op_timers.setdefault(name, []).append((a, b))
+        return r
 
     # -- initial state (initialization.py:278-414) --
     def init_state(self, current_time=0.0):
@@ -205,15 +218,18 @@ class Plane2d3vPlasmaSolver:
         Fp, Ff = self.fields[p], self.fields[f]
         cp, cf = self.currents[p], self.currents[f]
         hA, hB = self.half
-        self._move_wo_fields(prev, full)
-        self._move_smart(Fp, prev, full)
-        self._deposit(full, cf)
-        self._compute_fields(Fp, Fp, cp, cf, rb_full, rb_prev, rb_div, None, hA)
-        self._move_smart(hA, prev, full)
-        self._deposit(full, cf)
-        self._compute_fields(hA, Fp, cp, cf, rb_full, rb_prev, rb_div, Ff, hB)
-        self._move_smart(hB, prev, full)
-        self._deposit(full, cf)
+        T = self._timed
+        T("move_wo_fields", self._move_wo_fields, prev, full)
+        T("move_smart", self._move_smart, Fp, prev, full)
+        T("deposit", self._deposit, full, cf)
+        T("compute_fields", self._compute_fields, Fp, Fp, cp, cf, rb_full, rb_prev,
+          rb_div, None, hA)
+        T("move_smart", self._move_smart, hA, prev, full)
+        T("deposit", self._deposit, full, cf)
+        T("compute_fields", self._compute_fields, hA, Fp, cp, cf, rb_full, rb_prev,
+          rb_div, Ff, hB)
+        T("move_smart", self._move_smart, hB, prev, full)
+        T("deposit", self._deposit, full, cf)
         self.cur = f
         self.last_fields = Fp
 

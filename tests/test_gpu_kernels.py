@@ -130,10 +130,11 @@ def test_deposit_runaway_particles_take_global_path(kat):
     out = [torch.zeros((2, N, N), dtype=torch.float64, device=DEV) for _ in range(4)]
     ws = torch.empty(256, dtype=torch.uint8, device=DEV)
     err = torch.zeros(1, dtype=torch.int32, device=DEV)
+    inputs = [T(a.ravel()) for a in (d["x_init"], d["y_init"], xo, yo, d["k2_px"],
+                                     d["k2_py"], d["k2_pz"], d["k2_q"], d["m"])]
     _lib.check(L.lcb_plasma_deposit(
-        Ns * Ns, 1, N, h, Ns, _lib.LCB_PREC_FP64, *(T(a.ravel()).data_ptr() for a in (
-            d["x_init"], d["y_init"], xo, yo, d["k2_px"], d["k2_py"], d["k2_pz"],
-            d["k2_q"], d["m"])), None, *(o.data_ptr() for o in out),
+        Ns * Ns, 1, N, h, Ns, _lib.LCB_PREC_FP64, *(t.data_ptr() for t in inputs),
+        None, *(o.data_ptr() for o in out),
         ws.data_ptr(), ws.numel(), err.data_ptr(), _lib.stream_handle()), "k3")
     torch.cuda.synchronize()
     assert int(err.item()) == 0
