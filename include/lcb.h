@@ -150,6 +150,30 @@ typedef struct lcb_compute_fields_args {
 int lcb_compute_fields(const lcb_compute_fields_args *a, void *stream);
 size_t lcb_compute_fields_workspace_bytes(int grid_steps, int precision);
 
+/* Allocation-free compute_fields.  No counterpart in the reference: it exists
+ * for callers that cannot allocate device memory themselves -- a host code
+ * that only receives device pointers from another framework's memory pool,
+ * or a language binding with no route to a CUDA allocator -- and so cannot
+ * provide the workspace lcb_compute_fields asks for.
+ *
+ * Same arguments and results as lcb_compute_fields, except that a->workspace
+ * and a->workspace_bytes are ignored: the scratch is a file-scope device
+ * array of LCB_NOALLOC_FIELDS_SCRATCH_BYTES bytes inside liblcb.so, held on
+ * every GPU that loads the library until the process exits.  Grids whose
+ * scratch need (lcb_compute_fields_workspace_bytes) exceeds it are rejected
+ * with LCB_ERR_INVALID; every odd grid_steps up to 263 fits in
+ * LCB_PREC_FP64 and up to 361 in LCB_PREC_MIXED.  Nothing is allocated or
+ * freed.
+ *
+ * The first call on a device looks up the array's device address there
+ * (cudaGetSymbolAddress, with that device current); make that first call
+ * before any stream capture.  All calls share the one array and find the
+ * previous call's contents in it; the solver clears what must start at zero
+ * itself.  Calls that overlap on the GPU (e.g. on two streams at once) race
+ * on the array and give wrong results: serialise them. */
+#define LCB_NOALLOC_FIELDS_SCRATCH_BYTES ((size_t)8 << 20)
+int lcb_compute_fields_noalloc(const lcb_compute_fields_args *a, void *stream);
+
 /* ---------------------------------------------------------------------
  * Beam
  * ------------------------------------------------------------------- */

@@ -65,6 +65,7 @@ _SIGS = {
     "lcb_plasma_deposit_workspace_bytes": (C.c_size_t, [_i, _i]),
     "lcb_compute_fields": (_i, [C.POINTER(ComputeFieldsArgs), _vp]),
     "lcb_compute_fields_workspace_bytes": (C.c_size_t, [_i, _i]),
+    "lcb_compute_fields_noalloc": (_i, [C.POINTER(ComputeFieldsArgs), _vp]),
     "lcb_beam_deposit": (_i, [_i64, _i, _d, _d, _i64] + [_vp] * 6 + [_vp, _vp]),
     "lcb_beam_substepping": (_i, [_i64, _vp, _vp, _d, _d, _vp, _vp, _vp]),
     "lcb_beam_move": (_i, [_i64, _d, _d, _i64, _d, _i, _vp, _vp,

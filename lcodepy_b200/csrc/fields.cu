@@ -522,3 +522,61 @@ extern "C" int lcb_compute_fields(const lcb_compute_fields_args *a, void *stream
     Ops<double> op{c.dst, c.dct, c.dctT, c.dirichlet, c.mixed, c.mixedT, c.neumann};
     return solve<double>(a, op, st);
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant: the scratch is a file-scope device array instead
+// of a caller-provided workspace (see lcb_compute_fields_noalloc in lcb.h).
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace lcb {
+
+static __device__ __align__(256) unsigned char g_fields_scratch[LCB_NOALLOC_FIELDS_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+static void *g_scratch_addr[kMaxDevices] = {};
+static std::mutex g_scratch_mu;
+
+// Device address of g_fields_scratch on the current device, looked up once
+// per device.  The host-side symbol is only a stand-in and must never be
+// handed to a kernel.
+static int scratch_address(void **out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_check(e, "cudaGetDevice");
+    if (dev < 0 || dev >= kMaxDevices) {
+        set_error("device ordinal %d out of range for the allocation-free path", dev);
+        return LCB_ERR_INVALID;
+    }
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (!g_scratch_addr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_fields_scratch);
+        if (e != cudaSuccess) return cuda_check(e, "cudaGetSymbolAddress(g_fields_scratch)");
+        g_scratch_addr[dev] = p;
+    }
+    *out = g_scratch_addr[dev];
+    return LCB_OK;
+}
+
+}  // namespace lcb
+
+extern "C" int lcb_compute_fields_noalloc(const lcb_compute_fields_args *a, void *stream)
+{
+    LCB_REQUIRE(a, "args is NULL");
+    const size_t need = lcb_compute_fields_workspace_bytes(a->grid_steps, a->precision);
+    LCB_REQUIRE(need > 0, "grid_steps must be odd and >= 5 (got %d)", a->grid_steps);
+    LCB_REQUIRE(need <= LCB_NOALLOC_FIELDS_SCRATCH_BYTES,
+                "grid_steps %d in precision %d needs %zu bytes of scratch; the "
+                "allocation-free entry point has %zu (largest grid: 263 in FP64, "
+                "361 in mixed precision) -- use lcb_compute_fields with a workspace",
+                a->grid_steps, a->precision, need, (size_t)LCB_NOALLOC_FIELDS_SCRATCH_BYTES);
+    void *scratch = nullptr;
+    int rc = scratch_address(&scratch);
+    if (rc) return rc;
+    lcb_compute_fields_args b = *a;
+    b.workspace = scratch;
+    b.workspace_bytes = LCB_NOALLOC_FIELDS_SCRATCH_BYTES;
+    return lcb_compute_fields(&b, stream);
+}
