@@ -38,10 +38,10 @@ WORKLOAD = "lcode3d-production-fp64: N=513 h=0.02 ppc=4 dxi=0.02 L=60 beam=1e6 b
 METRIC = "xi-steps*cells/s"
 
 
-def workload_config(precision="fp64"):
+def workload_config(precision="fp64", window_length=60.0):
     return {'geometry': '3d', 'processing-unit-type': 'gpu',
             'window-width': 5.13, 'transverse-step': 0.02,
-            'window-length': 60.0, 'xi-step': 0.02,
+            'window-length': window_length, 'xi-step': 0.02,
             'time-limit': 1.0, 'time-step': 1.0,
             'ion-model': 'background', 'plasma-particles-per-cell': 4,
             'rigid-beam': False, 'print-every': 0, 'precision': precision}
@@ -163,7 +163,7 @@ def run_gpu(args, ws, rank, local):
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    cfg = workload_config(args.precision)
+    cfg = workload_config(args.precision, args.window_length)
     beam_host = make_beam()
     sim = Simulation(config=cfg, beam_parameters={}, runas_filename='')
     ps = sim.push_solver
@@ -217,7 +217,7 @@ def run_gpu(args, ws, rank, local):
         ops[name] = {"launches": len(evs), "ms_total": tot, "ms_avg": tot / max(len(evs), 1)}
 
     # ---- end to end through the public API, host buffers in and out ----
-    e2e = run_e2e(cfg, beam_host, dev)
+    e2e = None if args.no_e2e else run_e2e(cfg, beam_host, dev)
 
     return dict(value=value, ms_per_step=ms_per_step, N=N, ops=ops,
                 launches=int(ev["l1"] - ev["l0"]), clocks=ev.get("clocks"),
@@ -282,6 +282,11 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=8,
                     help="xi steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true",
+                    help="skip the end-to-end Simulation run (profiling runs)")
+    ap.add_argument("--window-length", type=float, default=60.0,
+                    help="xi window length; smaller values give the small "
+                         "profiling case of the same grid and beam")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
@@ -332,11 +337,14 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64" if args.precision == "fp64" else "f64-particles/f32-fields",
                 "data": "synthetic (seeded bi-Gaussian beam, uniform plasma)",
-                "config": {"workload": WORKLOAD, "grid": N, "xi_iterations": r["n_iter"],
+                "config": {"workload": WORKLOAD if args.window_length == 60.0 else
+                           WORKLOAD.replace("L=60", f"L={args.window_length:g}"),
+                           "grid": N, "xi_iterations": r["n_iter"],
                            "precision": args.precision, "parallelism": "replicas",
                            "l2": "inputs larger than L2 (no flush)"},
-                "e2e": {k: r["e2e"][k] for k in ("value", "unit", "h2d_bytes_per_step",
-                                                 "d2h_bytes_per_step")},
+                "e2e": (None if r["e2e"] is None else
+                        {k: r["e2e"][k] for k in ("value", "unit", "h2d_bytes_per_step",
+                                                  "d2h_bytes_per_step")}),
                 "gpu_launches": r["launches"], "clocks": r["clocks"],
                 "roofline": roof, "cpu_baseline": cpu,
                 "ops": {k: {"launches": v["launches"], "ms_avg": round(v["ms_avg"], 5),

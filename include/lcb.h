@@ -101,20 +101,19 @@ size_t lcb_plasma_deposit_workspace_bytes(int grid_steps, int precision);
  * Field solver
  * ------------------------------------------------------------------- */
 
-/* Constant operators, built once on the host and uploaded (FP64):
- *   dst  (N-2)x(N-2): 2 sin(pi (j+1)(k+1) / (N-1))        DST-I
- *   dct  N x N      : c_j cos(pi j k / (N-1)), c = 1,2..2,1 DCT-I (rows k)
- *   dctT N x N      : its transpose
- *   dirichlet (N-2)^2, mixed (N-2)xN, mixedT Nx(N-2), neumann NxN: the
- *   reference's solver matrices (lcode/plasma3d/initialization.py:15-67).
- * For LCB_PREC_MIXED the same operators are also given in FP32 (the *_f
- * pointers); they may be NULL in FP64 mode. */
-typedef struct lcb_field_consts {
-    const double *dst, *dct, *dctT;
-    const double *dirichlet, *mixed, *mixedT, *neumann;
-    const float *dst_f, *dct_f, *dctT_f;
-    const float *dirichlet_f, *mixed_f, *mixedT_f, *neumann_f;
-} lcb_field_consts;
+/* Constant operators of the field solver, built once per grid on the device
+ * by lcb_field_operators_build into a caller buffer of
+ * lcb_field_operators_bytes(N, precision) bytes (256-byte aligned): the
+ * even/odd halves of the DST-I matrix 2 sin(pi (j+1)(k+1)/(N-1)) (order N-2)
+ * and of the DCT-I matrix c_j cos(pi j k/(N-1)) (order N), and the
+ * reference's Dirichlet, mixed (and its transpose) and Neumann solver
+ * matrices (lcode/plasma3d/initialization.py:15-67), in FP64, or in FP32
+ * for LCB_PREC_MIXED.  subtraction_coeff is the Helmholtz shift of the mixed
+ * matrix ('field-solver-subtraction-coefficient' after the 3D adjustment). */
+size_t lcb_field_operators_bytes(int grid_steps, int precision);
+int lcb_field_operators_build(int grid_steps, double h, double subtraction_coeff,
+                              int precision, void *operators, size_t bytes,
+                              void *stream);
 
 /* Seven N x N planes in the order Ex, Ey, Ez, Bx, By, Bz, Phi. */
 typedef struct lcb_fields {
@@ -131,7 +130,8 @@ typedef struct lcb_compute_fields_args {
     int grid_steps;
     double h, xi_step, subtraction_coeff;
     int precision;
-    lcb_field_consts consts;
+    const void *operators;   /* from lcb_field_operators_build (same N, h,
+                                coefficient and precision) */
     lcb_fields fields;       /* Ex, Ey, Bx, By read (Helmholtz term) */
     lcb_fields fields_prev;  /* read */
     lcb_currents currents_prev, currents_full;
@@ -146,7 +146,8 @@ typedef struct lcb_compute_fields_args {
 /* Replaces compute_fields, lcode/plasma3d/fields.py:276-322 (with
  * calculate_Ex_Ey_Bx_By :176-230, calculate_Ez :112-139, calculate_Bz
  * :233-266, calculate_Phi :142-159 and the GPU transforms :36-107): every
- * DST-I / DCT-I / mixed transform is a dense batched matrix product. */
+ * DST-I / DCT-I / mixed transform is a dense batched matrix product.
+ * Phi is skipped when both its out_full and out_half planes are NULL. */
 int lcb_compute_fields(const lcb_compute_fields_args *a, void *stream);
 size_t lcb_compute_fields_workspace_bytes(int grid_steps, int precision);
 
@@ -161,8 +162,8 @@ size_t lcb_compute_fields_workspace_bytes(int grid_steps, int precision);
  * array of LCB_NOALLOC_FIELDS_SCRATCH_BYTES bytes inside liblcb.so, held on
  * every GPU that loads the library until the process exits.  Grids whose
  * scratch need (lcb_compute_fields_workspace_bytes) exceeds it are rejected
- * with LCB_ERR_INVALID; every odd grid_steps up to 263 fits in
- * LCB_PREC_FP64 and up to 361 in LCB_PREC_MIXED.  Nothing is allocated or
+ * with LCB_ERR_INVALID; every odd grid_steps up to 261 fits in
+ * LCB_PREC_FP64 and up to 359 in LCB_PREC_MIXED.  Nothing is allocated or
  * freed.
  *
  * The first call on a device looks up the array's device address there

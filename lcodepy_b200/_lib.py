@@ -29,13 +29,6 @@ class LcbError(RuntimeError):
     """A liblcb call returned an error status."""
 
 
-class FieldConsts(C.Structure):
-    _fields_ = [(n, _vp) for n in (
-        "dst", "dct", "dctT", "dirichlet", "mixed", "mixedT", "neumann",
-        "dst_f", "dct_f", "dctT_f", "dirichlet_f", "mixed_f", "mixedT_f",
-        "neumann_f")]
-
-
 class Fields7(C.Structure):
     _fields_ = [("f", _vp * 7)]
 
@@ -47,7 +40,7 @@ class Currents4(C.Structure):
 class ComputeFieldsArgs(C.Structure):
     _fields_ = [
         ("grid_steps", _i), ("h", _d), ("xi_step", _d), ("subtraction_coeff", _d),
-        ("precision", _i), ("consts", FieldConsts), ("fields", Fields7),
+        ("precision", _i), ("operators", _vp), ("fields", Fields7),
         ("fields_prev", Fields7), ("currents_prev", Currents4),
         ("currents_full", Currents4), ("rho_beam_full", _vp), ("rho_beam_prev", _vp),
         ("rho_beam_divisor", _d), ("out_full", Fields7), ("out_half", Fields7),
@@ -63,6 +56,8 @@ _SIGS = {
     "lcb_plasma_deposit": (_i, [_i64, _i, _i, _d, _i, _i] + [_vp] * 14 +
                            [_vp, C.c_size_t, _vp, _vp]),
     "lcb_plasma_deposit_workspace_bytes": (C.c_size_t, [_i, _i]),
+    "lcb_field_operators_bytes": (C.c_size_t, [_i, _i]),
+    "lcb_field_operators_build": (_i, [_i, _d, _d, _i, _vp, C.c_size_t, _vp]),
     "lcb_compute_fields": (_i, [C.POINTER(ComputeFieldsArgs), _vp]),
     "lcb_compute_fields_workspace_bytes": (C.c_size_t, [_i, _i]),
     "lcb_compute_fields_noalloc": (_i, [C.POINTER(ComputeFieldsArgs), _vp]),

@@ -140,11 +140,32 @@ k_move_smart(int64_t n, double xi_step, double boundary, double h, int N,
 // particle (a runaway, a lattice that is not a lattice) goes straight to
 // global atomics.  The window is then flushed with one global atomic per
 // non-zero cell and quantity.  The window origin follows the tile's first
-// particle's *initial* position, with S cells of slack for drift.
+// particle's initial position, with S cells of slack for drift.
+//
+// FP64 shared atomics retry when two lanes of a warp hit the same address in
+// the same instruction.  With two particles per cell along each axis (the
+// 2 x 2 per cell lattice) the lanes of a warp are therefore given particles of
+// one parity sub-lattice (every other row and column), which sit in distinct
+// cells; all 25 stencil points of a warp instruction then differ too.
 // ---------------------------------------------------------------------------
 constexpr int DEP_TI = 16, DEP_TJ = 32, DEP_THREADS = 256;
+constexpr int DEP_NP = DEP_TI * DEP_TJ;
+constexpr int DEP_PPT = DEP_NP / DEP_THREADS;
 constexpr int DEP_SLACK = 4;
 constexpr int DEP_WX = 28, DEP_WY = 44;  // >= tile cells (fineness 1) + 4 + 2*slack
+
+// Tile position (ti, tj) of the q-th particle slot of a block.
+__device__ __forceinline__ void tile_slot(int q, bool two_per_cell, int &ti, int &tj)
+{
+    if (two_per_cell) {
+        const int par = q >> 7, w = q & 127;        // 4 parity sub-lattices of 8 x 16
+        ti = 2 * (w >> 4) + (par >> 1);
+        tj = 2 * (w & 15) + (par & 1);
+    } else {
+        ti = q / DEP_TJ;
+        tj = q % DEP_TJ;
+    }
+}
 
 template <typename Acc>
 __global__ void __launch_bounds__(DEP_THREADS)
@@ -172,10 +193,18 @@ k_deposit_tiled(int64_t n_per_sort, int Ns, int N, double h,
     const int64_t k0 = base + (int64_t)i0 * Ns + j0;
     const int wx0 = cell_of(x_init[k0] / h + 0.5, half_n, dummy) - 2 - DEP_SLACK;
     const int wy0 = cell_of(y_init[k0] / h + 0.5, half_n, dummy) - 2 - DEP_SLACK;
+    // lattice spacing along x: two particles per cell?
+    bool two = false;
+    if (i0 + 1 < Ns) {
+        const double d = x_init[k0 + Ns] - x_init[k0];
+        two = fabs(2 * d - h) < 0.25 * h;
+    }
     __syncthreads();
 
-    const int tj = threadIdx.x % DEP_TJ;
-    for (int ti = threadIdx.x / DEP_TJ; ti < DEP_TI; ti += DEP_THREADS / DEP_TJ) {
+#pragma unroll
+    for (int r = 0; r < DEP_PPT; r++) {
+        int ti, tj;
+        tile_slot(threadIdx.x + r * DEP_THREADS, two, ti, tj);
         const int i = i0 + ti, j = j0 + tj;
         if (i >= Ns || j >= Ns) continue;
         const int64_t k = base + (int64_t)i * Ns + j;
@@ -237,6 +266,12 @@ k_deposit_tiled(int64_t n_per_sort, int Ns, int N, double h,
         if (v2 != Acc(0)) atomicAdd(gjy + c, v2);
         if (v3 != Acc(0)) atomicAdd(gjz + c, v3);
     }
+}
+
+template <typename T>
+static size_t deposit_smem_bytes()
+{
+    return (size_t)4 * DEP_WX * DEP_WY * sizeof(T);
 }
 
 __global__ void k_f32_to_f64(int64_t n, const float *__restrict__ a, double *__restrict__ b)
@@ -326,11 +361,12 @@ extern "C" int lcb_plasma_deposit(
         dim3 grid((particles_side + DEP_TJ - 1) / DEP_TJ,
                   (particles_side + DEP_TI - 1) / DEP_TI, n_sorts);
         if (precision == LCB_PREC_FP64) {
-            const size_t sm = 4 * DEP_WX * DEP_WY * sizeof(double);
+            const size_t sm = deposit_smem_bytes<double>();
             static bool attr = false;
             if (!attr) {
-                cudaFuncSetAttribute(k_deposit_tiled<double>,
+                cudaError_t e = cudaFuncSetAttribute(k_deposit_tiled<double>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+                if (e != cudaSuccess) return cuda_check(e, "deposit smem attribute");
                 attr = true;
             }
             k_deposit_tiled<double><<<grid, DEP_THREADS, sm, st>>>(
@@ -343,7 +379,14 @@ extern "C" int lcb_plasma_deposit(
             float *w = static_cast<float *>(workspace);
             cudaError_t e = cudaMemsetAsync(w, 0, 8 * plane * sizeof(float), st);
             if (e != cudaSuccess) return cuda_check(e, "memset f32 currents");
-            const size_t sm = 4 * DEP_WX * DEP_WY * sizeof(float);
+            const size_t sm = deposit_smem_bytes<float>();
+            static bool attr_f = false;
+            if (!attr_f) {
+                e = cudaFuncSetAttribute(k_deposit_tiled<float>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+                if (e != cudaSuccess) return cuda_check(e, "deposit smem attribute");
+                attr_f = true;
+            }
             k_deposit_tiled<float><<<grid, DEP_THREADS, sm, st>>>(
                 n_per_sort, particles_side, N, h, x_init, y_init, x_offt, y_offt,
                 px, py, pz, q, m, w, w + 2 * plane, w + 4 * plane, w + 6 * plane, err);

@@ -14,7 +14,8 @@ Device layout (HBM, FP64, C order):
              half-step scratch sets;
   currents   ro jx jy jz, each (2, N, N) (plane = sort; background ions put
              ro_initial in plane 1), prev and full;
-  operators  DST-I / DCT-I matrices and the solver matrices (+ FP32 copies).
+  operators  folded DST-I / DCT-I blocks and the solver matrices, FP64 (or
+             FP32 in mixed precision), built by lcb_field_operators_build.
 """
 from __future__ import annotations
 
@@ -35,68 +36,27 @@ PARTICLE_NAMES = ("x_init", "y_init", "x_offt", "y_offt", "px", "py", "pz", "q",
 
 
 # ---------------------------------------------------------------------------
-# Solver matrices (initialization.py:15-67) and transform operators.
+# Field solver operators (initialization.py:15-67 and the DST-I / DCT-I
+# matrices of fields.py:16-31), built on the device.
 # ---------------------------------------------------------------------------
 
-def _lam(k, N, h):
-    return 4 / h ** 2 * np.sin(k * np.pi / (2 * (N - 1))) ** 2
-
-
-def dirichlet_matrix(N, h):
-    lam = _lam(np.arange(1, N - 1), N, h)
-    return 1 / (lam[:, None] + lam[None, :]) / (2 * (N - 1)) ** 2
-
-
-def mixed_matrix(N, h, c):
-    li, lj = _lam(np.arange(1, N - 1), N, h), _lam(np.arange(N), N, h)
-    return 1 / (li[:, None] + lj[None, :] + c) / (2 * (N - 1)) ** 2
-
-
-def neumann_matrix(N, h):
-    lam = _lam(np.arange(N), N, h)
-    with np.errstate(divide="ignore"):
-        mul = 1 / (lam[:, None] + lam[None, :])
-    mul[0, 0] = 0  # the zero mode only shifts Bz, whose mean is removed
-    return mul / (2 * (N - 1)) ** 2
-
-
-def dst1_matrix(n):
-    """Unnormalised DST-I of length n as a matrix: 2 sin(pi (j+1)(k+1)/(n+1))."""
-    k = np.arange(1, n + 1)
-    return 2 * np.sin(np.pi * np.outer(k, k) / (n + 1))
-
-
-def dct1_matrix(N):
-    """Unnormalised DCT-I of length N: y_k = sum_j c_j x_j cos(pi j k/(N-1)),
-    c_0 = c_{N-1} = 1, else 2."""
-    j = np.arange(N)
-    c = np.full(N, 2.0)
-    c[0] = c[-1] = 1.0
-    return np.cos(np.pi * np.outer(j, j) / (N - 1)) * c[None, :]
-
-
 class FieldOperators:
-    """Device copies of every constant operator the field solver needs."""
+    """The field solver's constant operators, built on the device by
+    liblcb (folded DST-I / DCT-I blocks and the solver matrices)."""
 
     def __init__(self, N, h, sub_coeff, device, mixed_precision):
-        n = N - 2
-        S = dst1_matrix(n)
-        Cm = dct1_matrix(N)
-        mats = {
-            "dst": S, "dct": Cm, "dctT": np.ascontiguousarray(Cm.T),
-            "dirichlet": dirichlet_matrix(N, h),
-            "mixed": mixed_matrix(N, h, sub_coeff),
-            "neumann": neumann_matrix(N, h),
-        }
-        mats["mixedT"] = np.ascontiguousarray(mats["mixed"].T)
-        self.t = {k: torch.tensor(np.ascontiguousarray(v), dtype=torch.float64, device=device)
-                  for k, v in mats.items()}
-        if mixed_precision:
-            for k in list(mats):
-                self.t[k + "_f"] = self.t[k].to(torch.float32)
-        self.struct = _lib.FieldConsts()
-        for k, v in self.t.items():
-            setattr(self.struct, k, v.data_ptr())
+        L = _lib.load()
+        self.precision = _lib.LCB_PREC_MIXED if mixed_precision else _lib.LCB_PREC_FP64
+        nbytes = L.lcb_field_operators_bytes(N, self.precision)
+        self.buf = torch.empty(nbytes, dtype=torch.uint8, device=device)
+        _lib.check(L.lcb_field_operators_build(N, h, sub_coeff, self.precision,
+                                               self.buf.data_ptr(), nbytes,
+                                               _lib.stream_handle()),
+                   "lcb_field_operators_build")
+
+    @property
+    def ptr(self):
+        return self.buf.data_ptr()
 
 
 # ---------------------------------------------------------------------------

@@ -184,7 +184,7 @@ class Plane2d3vPlasmaSolver:
         a = _lib.ComputeFieldsArgs()
         a.grid_steps, a.h, a.xi_step = self.N, self.h, self.dxi
         a.subtraction_coeff, a.precision = self.sub_coeff, self.precision
-        a.consts = self.ops.struct
+        a.operators = self.ops.ptr
         a.fields, a.fields_prev = F.struct, Fprev.struct
         a.currents_prev, a.currents_full = cprev.struct, cfull.struct
         a.rho_beam_full, a.rho_beam_prev = rb_full.data_ptr(), rb_prev.data_ptr()

@@ -153,7 +153,7 @@ def _fields_args(d, precision, ops, outs, ws):
     a = _lib.ComputeFieldsArgs()
     a.grid_steps, a.h, a.xi_step = N, float(d["h"]), float(d["dxi"])
     a.subtraction_coeff, a.precision = float(d["sub"]), precision
-    a.consts = ops.struct
+    a.operators = ops.ptr
     for i, k in enumerate(("Ex", "Ey", "Ez", "Bx", "By", "Bz", "Phi")):
         a.fields.f[i] = t(d["in_" + k])
         a.fields_prev.f[i] = t(d["prev_" + k])
@@ -308,3 +308,42 @@ def test_beam_move_vs_oracle():
         for k in ("x", "y", "xi", "px", "py", "pz"):
             close(N_(g[k])[idx], getattr(ref, k), 1e-11, k)
     assert lost.size > 0 and moved.size > 0 and fell.size > 0
+
+
+def _op_layout(N):
+    n = N - 2
+    se, so, ce, co = (n + 1) // 2, (n - 1) // 2, (N + 1) // 2, (N - 1) // 2
+    shapes = [(se, se), (so, so), (se, se), (so, so), (ce, ce), (co, co), (ce, ce), (co, co),
+              (n, n), (n, N), (N, n), (N, N)]
+    offs, lds, o = [], [], 0
+    for i, (r, c) in enumerate(shapes):
+        ld = (c + 1) // 2 * 2 if i < 8 else c   # transform blocks: even row stride
+        offs.append(o)
+        lds.append(ld)
+        o += (r * ld + 31) // 32 * 32
+    return shapes, offs, lds
+
+
+@pytest.mark.parametrize("N,mixed", [(33, False), (129, False), (65, True)])
+def test_field_operators_build(N, mixed):
+    """Device-built folded DST-I/DCT-I blocks and solver matrices against numpy."""
+    from scipy import fft as sfft
+    h, c = 0.05, 1.05
+    ops = FieldOperators(N, h, c, DEV, mixed)
+    torch.cuda.synchronize()
+    dt = np.float32 if mixed else np.float64
+    buf = ops.buf.cpu().numpy().view(dt)
+    n = N - 2
+    S = sfft.dst(np.eye(n), type=1, axis=0)   # column j = DST-I of e_j
+    Cm = sfft.dct(np.eye(N), type=1, axis=0)
+    blocks = [S[0::2, :(n + 1) // 2], S[1::2, :(n - 1) // 2]]
+    blocks += [blocks[0].T, blocks[1].T]
+    cb = [Cm[0::2, :(N + 1) // 2], Cm[1::2, :(N - 1) // 2]]
+    blocks += cb + [cb[0].T, cb[1].T]
+    blocks += [O.dirichlet_matrix(N, h), O.mixed_matrix(N, h, c), O.mixed_matrix(N, h, c).T,
+               O.neumann_matrix(N, h)]
+    shapes, offs, lds = _op_layout(N)
+    rel = 1e-6 if mixed else 1e-13
+    for i, (ref, shp, off, ld) in enumerate(zip(blocks, shapes, offs, lds)):
+        got = buf[off:off + shp[0] * ld].reshape(shp[0], ld)[:, :shp[1]].astype(np.float64)
+        close(got, ref, rel, f"operator block {i}")

@@ -47,7 +47,7 @@ def _inputs(N, seed):
 def _args(N, h, dxi, ops, inp, out_full, out_half, ws=None):
     a = _lib.ComputeFieldsArgs()
     a.grid_steps, a.h, a.xi_step, a.subtraction_coeff, a.precision = N, h, dxi, 1 + dxi, 0
-    a.consts = ops.struct
+    a.operators = ops.ptr
     for i in range(7):
         a.fields.f[i] = inp["F"][i].data_ptr()
         a.fields_prev.f[i] = inp["Fp"][i].data_ptr()
