@@ -190,7 +190,10 @@ def run_gpu(args, ws, rank, local):
             ev["l0"] = _lib.launch_count()
             ev["t0"] = torch.cuda.Event(enable_timing=True)
             ev["t0"].record()
-            ps.plasma_solver.op_timers = op_times
+        if W <= k < W + K:
+            # every 16th timed step runs eagerly with per-op CUDA events (the
+            # kernels are the same; the others replay the captured graphs)
+            ps.plasma_solver.op_timers = op_times if (k - W) % 16 == 0 else None
         if k == W + K:
             ev["t1"] = torch.cuda.Event(enable_timing=True)
             ev["t1"].record()

@@ -211,6 +211,54 @@ int lcb_beam_move(int64_t n, double xi_step, double r_max,
                   double *xi, double *px, double *py, double *pz,
                   uint8_t *flags, int *err, void *stream);
 
+/* Beam particles as SoA arrays (lcode/beam3d/data.py:21-60): xi x y px py pz
+ * q_m q_norm (FP64), id (int64), dt (FP64), remaining_steps (int64). */
+typedef struct lcb_beam_soa {
+    double *xi, *x, *y, *px, *py, *pz, *q_m, *q_norm;
+    int64_t *id;
+    double *dt;
+    int64_t *remaining_steps;
+} lcb_beam_soa;
+
+typedef struct lcb_beam_step_args {
+    int grid_steps;
+    double h, xi_step, r_max, substep_energy, time_step;
+    int64_t layer_idx;                 /* plasma layer i just computed: the push
+                                          moves layer i-1 between planes i-1, i */
+    int64_t layout_idx;                /* layer deposited into ro0 / ro1 */
+    lcb_beam_soa source;               /* beam sorted by xi, descending */
+    int64_t layout_begin, layout_end;  /* slice of source deposited (layer layout_idx) */
+    int64_t move_begin, move_end;      /* slice of source pushed (layer i-1, fresh) */
+    lcb_beam_soa fell_in;              /* particles that fell from the last push */
+    const int64_t *fell_in_count;      /* device */
+    lcb_beam_soa fell_out;             /* written: particles falling now */
+    int64_t *fell_out_count;           /* device, overwritten */
+    int64_t fell_capacity;
+    lcb_beam_soa drain;                /* moved particles are appended */
+    int64_t *drain_count;              /* device, advanced */
+    int64_t drain_capacity;
+    lcb_beam_soa lost;                 /* lost particles appended; all NULL: dropped */
+    int64_t *lost_count;               /* device, advanced (may be NULL if dropped) */
+    int64_t lost_capacity;
+    lcb_beam_soa stage;                /* scratch, >= fresh + fell particles */
+    uint8_t *stage_flags;
+    int64_t stage_capacity;
+    double *ro0, *ro1;                 /* beam density: this step's and the next */
+    const lcb_fields *fields_k, *fields_k1;  /* previous and new plasma fields */
+    int *err;
+} lcb_beam_step_args;
+
+/* One xi step of the beam with every count kept on the device: deposit the
+ * layout layer, push layer i-1 (fresh particles get their substep sizes
+ * first) followed by the particles that fell from the previous push, then
+ * compact in order: moved -> drain, fell -> fell_out, lost -> lost.  The
+ * deposit only reads the source, so a caller may lay out layer i+1 right
+ * after the plasma step of layer i.  Replaces the per-layer
+ * body of PusherAndSolver3D.step_dt for a non-rigid beam,
+ * lcode/push_solvers/push_solver.py:506-531 (layout_beam_layer,
+ * move_beam_layer, create_next_layer, push_beam_layer). */
+int lcb_beam_step(const lcb_beam_step_args *a, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

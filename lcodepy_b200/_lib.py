@@ -37,6 +37,26 @@ class Currents4(C.Structure):
     _fields_ = [("ro", _vp), ("jx", _vp), ("jy", _vp), ("jz", _vp), ("n_planes", _i)]
 
 
+class BeamSoA(C.Structure):
+    _fields_ = [(n, _vp) for n in ("xi", "x", "y", "px", "py", "pz", "q_m", "q_norm",
+                                   "id", "dt", "remaining_steps")]
+
+
+class BeamStepArgs(C.Structure):
+    _fields_ = [
+        ("grid_steps", _i), ("h", _d), ("xi_step", _d), ("r_max", _d),
+        ("substep_energy", _d), ("time_step", _d), ("layer_idx", _i64),
+        ("layout_idx", _i64),
+        ("source", BeamSoA), ("layout_begin", _i64), ("layout_end", _i64),
+        ("move_begin", _i64), ("move_end", _i64),
+        ("fell_in", BeamSoA), ("fell_in_count", _vp),
+        ("fell_out", BeamSoA), ("fell_out_count", _vp), ("fell_capacity", _i64),
+        ("drain", BeamSoA), ("drain_count", _vp), ("drain_capacity", _i64),
+        ("lost", BeamSoA), ("lost_count", _vp), ("lost_capacity", _i64),
+        ("stage", BeamSoA), ("stage_flags", _vp), ("stage_capacity", _i64),
+        ("ro0", _vp), ("ro1", _vp), ("fields_k", _vp), ("fields_k1", _vp), ("err", _vp)]
+
+
 class ComputeFieldsArgs(C.Structure):
     _fields_ = [
         ("grid_steps", _i), ("h", _d), ("xi_step", _d), ("subtraction_coeff", _d),
@@ -63,6 +83,7 @@ _SIGS = {
     "lcb_compute_fields_noalloc": (_i, [C.POINTER(ComputeFieldsArgs), _vp]),
     "lcb_beam_deposit": (_i, [_i64, _i, _d, _d, _i64] + [_vp] * 6 + [_vp, _vp]),
     "lcb_beam_substepping": (_i, [_i64, _vp, _vp, _d, _d, _vp, _vp, _vp]),
+    "lcb_beam_step": (_i, [C.POINTER(BeamStepArgs), _vp]),
     "lcb_beam_move": (_i, [_i64, _d, _d, _i64, _d, _i, _vp, _vp,
                            C.POINTER(Fields7), C.POINTER(Fields7)] + [_vp] * 9 + [_vp, _vp]),
 }
@@ -97,8 +118,19 @@ def check(rc: int, what: str):
         raise LcbError(f"{what} failed (status {rc}): {msg}")
 
 
+_replayed = 0
+
+
+def add_replayed(n: int):
+    """Count kernel launches made by replaying captured CUDA graphs (the
+    library's own counter sees each kernel once, at capture)."""
+    global _replayed
+    _replayed += n
+
+
 def launch_count() -> int:
-    return int(load().lcb_launch_count())
+    """liblcb kernel launches so far, direct and through graph replays."""
+    return int(load().lcb_launch_count()) + _replayed
 
 
 def ptr(t) -> int | None:

@@ -8,6 +8,8 @@ device reduction and a host sync per layer, beam3d/beam_io.py:29-47).
 """
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 import torch
 
@@ -124,6 +126,24 @@ class BeamSource:
         length = hi - lo
         return self.head, self.head + length
 
+    def all_layer_bounds(self, first=0, last=None):
+        """Slices of every layer the xi loop will cut, in order, as the
+        reference's successive get_beam_layer_to_layout calls would cut them
+        (count in range, then cut from the head)."""
+        out = {}
+        head = self.head
+        # deepest layer holding a particle: ceil(-min(xi) / dxi)
+        n_layers = last if last is not None else int(np.ceil(
+            max(float(self._neg_xi[-1]) if self._neg_xi.size else 0.0, 0.0) / self.dxi)) + 2
+        saved = self.head
+        for i in range(first, n_layers + 1):
+            self.head = head
+            a, b = self.layer_bounds(i)
+            out[i] = (a, b)
+            head = b
+        self.head = saved
+        return out
+
     def get_beam_layer_to_layout(self, layer_idx) -> BeamParticles:
         a, b = self.layer_bounds(layer_idx)
         self.head = b
@@ -187,12 +207,23 @@ class RigidBeamDrain:
         return None
 
 
+def _soa(b: "BeamParticles", offset: int = 0) -> "_lib.BeamSoA":
+    s = _lib.BeamSoA()
+    for k in BEAM_KEYS + ("dt", "remaining_steps"):
+        t = getattr(b, k)
+        setattr(s, k, t.data_ptr() + offset * t.element_size())
+    return s
+
+
 class BeamCalculator:
     """Beam density layout and push (beam_calculator.py:51-143), on the device.
 
-    Beam density planes stay undivided in HBM (the 1/h^2 of
-    beam_calculator.py:91 is applied by the field solver, which receives the
-    divisor), so ``rho_divisor`` must accompany any plane handed out."""
+    One xi step of the beam is one lcb_beam_step call: the push of layer i-1
+    (between the previous and the new plasma fields) and the layout of layer
+    i+1 for the next step, with every particle count kept on the device
+    (drain, fell and lost buffers with device counters).  Beam density planes
+    stay undivided in HBM (the 1/h^2 of beam_calculator.py:91 is applied by
+    the field solver, which receives ``rho_divisor``)."""
 
     def __init__(self, config: Config, device=None):
         self.device = device or torch.device("cuda", torch.cuda.current_device())
@@ -206,65 +237,106 @@ class BeamCalculator:
         self.rho_divisor = self.h ** 2
         self.planes = torch.zeros(3, self.N, self.N, dtype=torch.float64, device=self.device)
         self.err = torch.zeros(1, dtype=torch.int32, device=self.device)
-        self.i = 0
+        # device counters: fell A, fell B, drain, lost
+        self.counts = torch.zeros(4, dtype=torch.int64, device=self.device)
+        self.cap = 0
 
-    def start_time_step(self):
+    def _ensure(self, n_total, max_layer):
+        cap = max(n_total, 1)
+        stage = cap + max(max_layer, 1)
+        if cap <= self.cap and stage <= self.stage_cap:
+            return
+        self.cap, self.stage_cap = cap, stage
+        self.drain = BeamParticles(self.device, cap)
+        self.lost = BeamParticles(self.device, cap)
+        self.fell = [BeamParticles(self.device, cap), BeamParticles(self.device, cap)]
+        self.stage = BeamParticles(self.device, stage)
+        self.flags = torch.zeros(stage, dtype=torch.uint8, device=self.device)
+
+    def start_time_step(self, source: "BeamSource"):
+        """Zero the planes and counters and lay out the first layer."""
+        self.source = source
+        self.bounds = source.all_layer_bounds()
+        n = source.beam.size
+        max_layer = max((b - a for a, b in self.bounds.values()), default=0)
+        self._ensure(n, max_layer)
         self.planes.zero_()
-        self.i = 0
+        self.counts.zero_()
+        self.err.zero_()
+        self.fell_cur = 0
 
-    def rho_prev(self):
-        return self.planes[(self.i - 1) % 3]
+    def layer_bounds(self, i):
+        return self.bounds.get(i, (0, 0))
 
-    def layout_beam_layer(self, layer: BeamParticles, layer_idx: int):
-        """Deposit a layer: xi_loc weights into this step's plane, 1 - xi_loc
-        into the next step's (weights.py:152-163).  Returns (full, prev)."""
-        self.i = layer_idx
-        full = self.planes[layer_idx % 3]
-        nxt = self.planes[(layer_idx + 1) % 3]
-        nxt.zero_()
-        if layer.size:
+    def rho(self, i):
+        """(full, prev) density planes of xi step i."""
+        return self.planes[i % 3], self.planes[(i - 1) % 3]
+
+    def _args(self, layer_idx, layout, move, fields_k, fields_k1):
+        a = _lib.BeamStepArgs()
+        a.grid_steps, a.h, a.xi_step, a.r_max = self.N, self.h, self.dxi, self.r_max
+        a.substep_energy, a.time_step = self.substep_energy, self.time_step
+        a.layer_idx = layer_idx
+        a.source = _soa(self.source.beam)
+        a.layout_begin, a.layout_end = layout
+        a.move_begin, a.move_end = move
+        fi, fo = self.fell_cur, 1 - self.fell_cur
+        a.fell_in = _soa(self.fell[fi])
+        a.fell_in_count = self.counts[fi].data_ptr()
+        a.fell_out = _soa(self.fell[fo])
+        a.fell_out_count = self.counts[fo].data_ptr()
+        a.fell_capacity = self.cap
+        a.drain = _soa(self.drain)
+        a.drain_count = self.counts[2].data_ptr()
+        a.drain_capacity = self.cap
+        a.lost = _soa(self.lost)
+        a.lost_count = self.counts[3].data_ptr()
+        a.lost_capacity = self.cap
+        a.stage = _soa(self.stage)
+        a.stage_flags = self.flags.data_ptr()
+        a.stage_capacity = self.stage_cap
+        a.ro0 = self.planes[layer_idx % 3].data_ptr()
+        a.ro1 = self.planes[(layer_idx + 1) % 3].data_ptr()
+        a.fields_k = C.addressof(fields_k.struct) if fields_k is not None else None
+        a.fields_k1 = C.addressof(fields_k1.struct) if fields_k1 is not None else None
+        a.err = self.err.data_ptr()
+        return a
+
+    def layout_first(self, i):
+        """Lay out layer i alone (before the first xi step)."""
+        lo = self.layer_bounds(i)
+        if lo[1] > lo[0]:
             L = _lib.load()
             _lib.check(L.lcb_beam_deposit(
-                layer.size, self.N, self.h, self.dxi, layer_idx,
-                layer.x.data_ptr(), layer.y.data_ptr(), layer.xi.data_ptr(),
-                layer.q_norm.data_ptr(), full.data_ptr(), nxt.data_ptr(),
+                lo[1] - lo[0], self.N, self.h, self.dxi, i,
+                self.source.beam.x[lo[0]:].data_ptr(), self.source.beam.y[lo[0]:].data_ptr(),
+                self.source.beam.xi[lo[0]:].data_ptr(), self.source.beam.q_norm[lo[0]:].data_ptr(),
+                self.planes[i % 3].data_ptr(), self.planes[(i + 1) % 3].data_ptr(),
                 self.err.data_ptr(), _lib.stream_handle()), "lcb_beam_deposit")
-        prev = self.planes[(layer_idx - 1) % 3] if layer_idx > 0 else self._zero()
-        return full, prev
 
-    def _zero(self):
-        if not hasattr(self, "_z"):
-            self._z = torch.zeros(self.N, self.N, dtype=torch.float64, device=self.device)
-        return self._z
+    def after_plasma_step(self, i, fields_prev, fields_new):
+        """Push layer i-1 (and the particles that fell from the last push)
+        between fields_prev and fields_new, then lay out layer i+1."""
+        self.planes[(i + 2) % 3].zero_()
+        a = self._args(i, self.layer_bounds(i + 1), self.layer_bounds(i - 1),
+                       fields_prev, fields_new)
+        a.layout_idx = i + 1
+        a.ro0 = self.planes[(i + 1) % 3].data_ptr()
+        a.ro1 = self.planes[(i + 2) % 3].data_ptr()
+        _lib.check(_lib.load().lcb_beam_step(C.byref(a), _lib.stream_handle()),
+                   "lcb_beam_step")
+        self.fell_cur = 1 - self.fell_cur
 
-    def move_beam_layer(self, layer: BeamParticles, fell_size: int, layer_idx: int,
-                        fields_k, fields_k1):
-        """Substep and push the layer between the previous (k) and new (k+1)
-        plasma planes; returns (lost, moved, fell) (beam_calculator.py:97-134)."""
-        n = layer.size
-        if n == 0:
-            e = BeamParticles(self.device)
-            return e, e, e
-        L = _lib.load()
-        fresh = n - fell_size
-        st = _lib.stream_handle()
-        if fresh > 0:
-            _lib.check(L.lcb_beam_substepping(
-                fresh, layer.q_m.data_ptr(), layer.pz.data_ptr(), self.substep_energy,
-                self.time_step, layer.dt.data_ptr(), layer.remaining_steps.data_ptr(), st),
-                "lcb_beam_substepping")
-        flags = torch.empty(n, dtype=torch.uint8, device=self.device)
-        _lib.check(L.lcb_beam_move(
-            n, self.dxi, self.r_max, layer_idx - 1, self.h, self.N,
-            layer.q_m.data_ptr(), layer.dt.data_ptr(), fields_k.struct, fields_k1.struct,
-            layer.remaining_steps.data_ptr(), layer.id.data_ptr(), layer.x.data_ptr(),
-            layer.y.data_ptr(), layer.xi.data_ptr(), layer.px.data_ptr(),
-            layer.py.data_ptr(), layer.pz.data_ptr(), flags.data_ptr(),
-            self.err.data_ptr(), st), "lcb_beam_move")
-        lost = layer.take((flags & 1) != 0)
-        moved = layer.take((flags & 2) != 0)
-        fell = layer.take((flags & 4) != 0)
-        return lost, moved, fell
+    def finish(self):
+        """Moved and lost particles of the time step (one host read)."""
+        c = self.counts.cpu().numpy()
+        out = []
+        for buf, n in ((self.drain, int(c[2])), (self.lost, int(c[3]))):
+            v = buf.take(slice(0, n))
+            for k in v._all():  # own the data: the buffers are reused next time step
+                setattr(v, k, getattr(v, k).clone())
+            out.append(v)
+        return out[0], out[1]
 
 
 class RigidBeamCalculator:

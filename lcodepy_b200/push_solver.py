@@ -15,8 +15,7 @@ from __future__ import annotations
 
 import torch
 
-from .beam3d import (BeamCalculator, BeamDrain, BeamParticles, BeamSource,
-                     RigidBeamCalculator)
+from .beam3d import BeamCalculator, RigidBeamCalculator
 from .config import Config
 from .data import Arrays
 from .solver import Plane2d3vPlasmaSolver
@@ -50,34 +49,27 @@ class PusherAndSolver3D:
         bc = self.beam_calculator
         N = self.grid_steps
         c = N // 2
-        bc.start_time_step()
         first = round(-xi_plasma_layer_start / self.xi_step_size) + 1
         last = self.xi_steps
         if self.rigid:
             bc.prepare(beam_source.get_beam_layer_to_layout(first), first, last)
+        else:
+            bc.start_time_step(beam_source)
+            bc.layout_first(first)
         n_iter = max(last - first + 1, 0)
         ez = torch.zeros(n_iter, dtype=torch.float64, device=self.device)
-        to_move = BeamParticles(self.device)
-        fell_size = 0
-        self.lost = []
+        self.lost = None
         for k, xi_i in enumerate(range(first, last + 1)):
             if step_hook is not None:
                 step_hook(k)
             if self.rigid:
                 rb_full, rb_prev = bc.layout_beam_layer(None, xi_i)
-                layer = None
             else:
-                layer = beam_source.get_beam_layer_to_layout(xi_i)
-                rb_full, rb_prev = bc.layout_beam_layer(layer, xi_i)
+                rb_full, rb_prev = bc.rho(xi_i)
             ps.step_dxi(rb_full, rb_prev, bc.rho_divisor)
             if not self.rigid:
-                lost, moved, fell = bc.move_beam_layer(to_move, fell_size, xi_i,
-                                                       ps.last_fields, ps.prev_fields)
-                to_move = layer.append(fell)
-                fell_size = fell.size
-                beam_drain.push_beam_layer(moved)
-                if lost.size:
-                    self.lost.append(lost)
+                # push layer i-1 between the previous and new fields, lay out i+1
+                bc.after_plasma_step(xi_i, ps.last_fields, ps.prev_fields)
             ez[k] = ps.prev_fields.Ez[c, c]
             if diagnostics_list:
                 xi_layer = -self.xi_step_size * xi_i
@@ -96,7 +88,10 @@ class PusherAndSolver3D:
             if e:
                 bc.err.zero_()
                 raise RuntimeError(f"beam device error word 0x{e:x}: a beam stencil "
-                                   "left the grid or a substep limit was hit")
+                                   "left the grid, a substep limit was hit or a beam "
+                                   "buffer would overflow")
+            moved, self.lost = bc.finish()
+            beam_drain.push_beam_layer(moved)
         self.ez_axis = ez
         if self.print_every:
             vals = ez.cpu().numpy()

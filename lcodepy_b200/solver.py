@@ -92,6 +92,16 @@ class Plane2d3vPlasmaSolver:
         self.cur = 0  # index of the "prev" copy in self.states / fields / currents
         # name -> list of (start, end) CUDA events, filled while not None
         self.op_timers = None
+        # CUDA graphs of one xi step, one per buffer parity; the beam density
+        # planes are copied into fixed buffers so the graphs stay valid.
+        pe = config.getraw('cuda-graphs')
+        self.use_graphs = True if pe is None else bool(pe)
+        self.rbf = torch.zeros(N, N, dtype=torch.float64, device=dev)
+        self.rbp = torch.zeros(N, N, dtype=torch.float64, device=dev)
+        self.graphs = [None, None]
+        self.graph_launches = [0, 0]
+        self.graph_div = None
+        self.eager_steps = 0
 
     def _timed(self, name, fn, *args):
         if self.op_timers is None:
@@ -140,6 +150,7 @@ class Plane2d3vPlasmaSolver:
             c.buf.zero_()
         self.err.zero_()
         self.cur = 0
+        self.last_fields = self.fields[1]
 
     # -- kernels --
     def _deposit(self, st: PlasmaState, out: CurrentSet, with_background=True, n_sorts=None):
@@ -212,7 +223,37 @@ class Plane2d3vPlasmaSolver:
     def step_dxi(self, rb_full: torch.Tensor, rb_prev: torch.Tensor, rb_div: float = 1.0):
         """Advance the plasma by one xi step; afterwards the new state is the
         "prev" state (fields / currents / particles) and the step's input
-        fields remain readable as ``last_fields`` until the next step."""
+        fields remain readable as ``last_fields`` until the next step.
+
+        After two eager steps the step runs as a captured CUDA graph (one per
+        parity of the rotating buffers), unless per-op timing is requested."""
+        if not self.use_graphs or self.op_timers is not None:
+            self._step_ops(rb_full, rb_prev, rb_div)
+            self.eager_steps += 1
+            return
+        self.rbf.copy_(rb_full)
+        self.rbp.copy_(rb_prev)
+        if self.graph_div != rb_div:
+            self.graphs = [None, None]
+            self.graph_div = rb_div
+        p = self.cur
+        if self.graphs[p] is None:
+            if self.eager_steps < 2:
+                self._step_ops(self.rbf, self.rbp, rb_div)
+                self.eager_steps += 1
+                return
+            g = torch.cuda.CUDAGraph()
+            n0 = _lib.load().lcb_launch_count()
+            with torch.cuda.graph(g):
+                self._step_ops(self.rbf, self.rbp, rb_div, advance=False)
+            self.graph_launches[p] = _lib.load().lcb_launch_count() - n0
+            self.graphs[p] = g
+        self.graphs[p].replay()
+        _lib.add_replayed(self.graph_launches[p])
+        self.cur = 1 - p
+        self.last_fields = self.fields[p]
+
+    def _step_ops(self, rb_full, rb_prev, rb_div, advance=True):
         p, f = self.cur, 1 - self.cur
         prev, full = self.states[p], self.states[f]
         Fp, Ff = self.fields[p], self.fields[f]
@@ -230,8 +271,9 @@ class Plane2d3vPlasmaSolver:
           rb_div, Ff, hB)
         T("move_smart", self._move_smart, hB, prev, full)
         T("deposit", self._deposit, full, cf)
-        self.cur = f
-        self.last_fields = Fp
+        if advance:
+            self.cur = f
+            self.last_fields = Fp
 
     # -- views with the reference's names --
     def particles_dict(self) -> dict:

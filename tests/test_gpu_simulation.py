@@ -144,3 +144,17 @@ def test_mixed_precision_on_axis_ez():
     l2 = np.linalg.norm(ezmx - ez64) / np.linalg.norm(ez64)
     print("mixed vs fp64 on-axis Ez rel L2:", l2)
     assert l2 < 1e-5
+
+
+@pytest.mark.parametrize("rigid", [True, False])
+def test_cuda_graphs_match_eager(rigid):
+    """The captured-graph xi step gives the eager step's results."""
+    extra = {'rigid-beam': True} if rigid else {'window-length': 1.5}
+    beam = rigid_driver if rigid else {'current': 0.05, 'particles_in_layer': 400,
+                                       'default': {'length': 2.0}}
+    _, p0, f0, c0, ez0 = run(cfg(**extra, **{'cuda-graphs': False}), beam)
+    sim, p1, f1, c1, ez1 = run(cfg(**extra, **{'cuda-graphs': True}), beam)
+    assert sim.push_solver.plasma_solver.graphs[0] is not None
+    assert rel_err(ez1, ez0) < 1e-12
+    for k in ("Ex", "Ey", "Ez", "Bx", "By", "Bz", "Phi"):
+        assert rel_err(getattr(f1, k).cpu().numpy(), getattr(f0, k).cpu().numpy()) < 1e-12, k
