@@ -97,6 +97,35 @@ int lcb_plasma_deposit(int64_t n_per_sort, int n_sorts, int grid_steps,
                        void *stream);
 size_t lcb_plasma_deposit_workspace_bytes(int grid_steps, int precision);
 
+/* Plasma particle arrays of all sorts (concatenated). */
+typedef struct lcb_plasma_particles {
+    double *x_init, *y_init, *x_offt, *y_offt, *px, *py, *pz, *q, *m;
+} lcb_plasma_particles;
+
+typedef struct lcb_move_deposit_args {
+    int64_t n_per_sort;
+    int n_sorts, particles_side, grid_steps, precision;
+    int first;               /* 1: first stage of an xi step (full estimated here) */
+    int lattice_fineness;    /* particles per cell along an axis (window size hint) */
+    double xi_step, boundary, h;
+    const double *fields[6]; /* Ex Ey Ez Bx By Bz used for the midpoint gather */
+    lcb_plasma_particles prev, full;  /* full.{x_offt,y_offt,px,py,pz,q} written */
+    const double *ro_initial;         /* background ions, or NULL */
+    double *ro, *jx, *jy, *jz;        /* (2, N, N) outputs, zeroed here */
+    void *workspace;                  /* lcb_plasma_deposit_workspace_bytes */
+    size_t workspace_bytes;
+    int *err;
+} lcb_move_deposit_args;
+
+/* One predictor-corrector stage fused: move_smart on every particle and the
+ * deposition of its new state, and for the first stage of an xi step the
+ * free-streaming estimate before them.  The results equal
+ * lcb_plasma_move_wo_fields (first stage) + lcb_plasma_move_smart +
+ * lcb_plasma_deposit.  Replaces, for one stage of
+ * Plane2d3vPlasmaSolver.step_dxi (lcode/plasma3d/solver.py:29-76), the calls
+ * move_particles_wo_fields / move_particles / compute_rhoj. */
+int lcb_plasma_move_deposit(const lcb_move_deposit_args *a, void *stream);
+
 /* ---------------------------------------------------------------------
  * Field solver
  * ------------------------------------------------------------------- */

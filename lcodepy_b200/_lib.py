@@ -37,6 +37,21 @@ class Currents4(C.Structure):
     _fields_ = [("ro", _vp), ("jx", _vp), ("jy", _vp), ("jz", _vp), ("n_planes", _i)]
 
 
+class PlasmaParticles(C.Structure):
+    _fields_ = [(n, _vp) for n in ("x_init", "y_init", "x_offt", "y_offt", "px", "py",
+                                   "pz", "q", "m")]
+
+
+class MoveDepositArgs(C.Structure):
+    _fields_ = [
+        ("n_per_sort", _i64), ("n_sorts", _i), ("particles_side", _i), ("grid_steps", _i),
+        ("precision", _i), ("first", _i), ("lattice_fineness", _i),
+        ("xi_step", _d), ("boundary", _d), ("h", _d), ("fields", _vp * 6),
+        ("prev", PlasmaParticles), ("full", PlasmaParticles), ("ro_initial", _vp),
+        ("ro", _vp), ("jx", _vp), ("jy", _vp), ("jz", _vp),
+        ("workspace", _vp), ("workspace_bytes", C.c_size_t), ("err", _vp)]
+
+
 class BeamSoA(C.Structure):
     _fields_ = [(n, _vp) for n in ("xi", "x", "y", "px", "py", "pz", "q_m", "q_norm",
                                    "id", "dt", "remaining_steps")]
@@ -76,6 +91,7 @@ _SIGS = {
     "lcb_plasma_deposit": (_i, [_i64, _i, _i, _d, _i, _i] + [_vp] * 14 +
                            [_vp, C.c_size_t, _vp, _vp]),
     "lcb_plasma_deposit_workspace_bytes": (C.c_size_t, [_i, _i]),
+    "lcb_plasma_move_deposit": (_i, [C.POINTER(MoveDepositArgs), _vp]),
     "lcb_field_operators_bytes": (C.c_size_t, [_i, _i]),
     "lcb_field_operators_build": (_i, [_i, _d, _d, _i, _vp, C.c_size_t, _vp]),
     "lcb_compute_fields": (_i, [C.POINTER(ComputeFieldsArgs), _vp]),

@@ -35,15 +35,19 @@ int sm_count();
 // ---- 4th-order spline weights at offsets -2..2 ----
 // The reference's weight4 (lcode/plasma3d/weights.py:13-31, :127-148),
 // evaluated for all five offsets at once.
+// Divisions by 6 and 24 are multiplications by the rounded reciprocals here
+// (at most an ulp from the reference's quotients; IEEE division would cost a
+// Newton sequence per term).
 __device__ __forceinline__ void weights4(double x, double w[5])
 {
+    constexpr double r6 = 1.0 / 6.0, r24 = 1.0 / 24.0;
     const double x2 = x * x, x3 = x2 * x, x4 = x3 * x;
     const double a = 0.5 - x, b = 0.5 + x;
-    w[0] = a * a * a * a / 24.;
-    w[1] = 19 / 96. - 11 / 24. * x + x2 / 4. + x3 / 6. - x4 / 6.;
-    w[2] = 115 / 192. - 5 / 8. * x2 + x4 / 4.;
-    w[3] = 19 / 96. + 11 / 24. * x + x2 / 4. - x3 / 6. - x4 / 6.;
-    w[4] = b * b * b * b / 24.;
+    w[0] = a * a * a * a * r24;
+    w[1] = 19 / 96. - 11 / 24. * x + x2 * 0.25 + x3 * r6 - x4 * r6;
+    w[2] = 115 / 192. - 5 / 8. * x2 + x4 * 0.25;
+    w[3] = 19 / 96. + 11 / 24. * x + x2 * 0.25 - x3 * r6 - x4 * r6;
+    w[4] = b * b * b * b * r24;
 }
 
 // Cell of a position (in cell units, already offset by +0.5) and the local

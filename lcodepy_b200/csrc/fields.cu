@@ -454,34 +454,33 @@ struct FoldBatch {
 template <typename T>
 __global__ void __launch_bounds__(256) k_fold(const __grid_constant__ FoldBatch<T> fb)
 {
+    // blockIdx.y: row, x: columns (grid-stride), z: problem
     const FoldDesc<T> &f = fb.d[blockIdx.z];
     const int R = f.R, C = f.C, ldc = ld2(C);
-    const int64_t total = (int64_t)R * C;
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
-         e += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(e / C), j = (int)(e % C);
-        if (!f.by_rows) {
-            const int he = (C + 1) / 2, mid = (C - 1) / 2;
-            const T *row = f.src + (int64_t)i * ldc;
-            if (j < he) {
-                const T v = j < mid ? row[j] + row[C - 1 - j] : row[mid];
-                f.dst[(int64_t)i * ld2(he) + j] = v;
+    for (int i = blockIdx.y; i < R; i += gridDim.y) {
+        for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < C; j += gridDim.x * blockDim.x) {
+            if (!f.by_rows) {
+                const int he = (C + 1) / 2, mid = (C - 1) / 2;
+                const T *row = f.src + (int64_t)i * ldc;
+                if (j < he) {
+                    f.dst[(int64_t)i * ld2(he) + j] = j < mid ? row[j] + row[C - 1 - j] : row[mid];
+                } else {
+                    const int jj = j - he;
+                    T *V = f.dst + (int64_t)R * ld2(he);
+                    V[(int64_t)i * ld2(C - he) + jj] = row[jj] - row[C - 1 - jj];
+                }
             } else {
-                const int jj = j - he;
-                T *V = f.dst + (int64_t)R * ld2(he);
-                V[(int64_t)i * ld2(C - he) + jj] = row[jj] - row[C - 1 - jj];
+                const int he = (R + 1) / 2, mid = (R - 1) / 2;
+                T v;
+                if (i < he) {
+                    v = i < mid ? f.src[(int64_t)i * ldc + j] + f.src[(int64_t)(R - 1 - i) * ldc + j]
+                                : f.src[(int64_t)mid * ldc + j];
+                } else {
+                    const int ii = i - he;
+                    v = f.src[(int64_t)ii * ldc + j] - f.src[(int64_t)(R - 1 - ii) * ldc + j];
+                }
+                f.dst[(int64_t)i * ldc + j] = v;
             }
-        } else {
-            const int he = (R + 1) / 2, mid = (R - 1) / 2;
-            T v;
-            if (i < he) {
-                v = i < mid ? f.src[(int64_t)i * ldc + j] + f.src[(int64_t)(R - 1 - i) * ldc + j]
-                            : f.src[(int64_t)mid * ldc + j];
-            } else {
-                const int ii = i - he;
-                v = f.src[(int64_t)ii * ldc + j] - f.src[(int64_t)(R - 1 - ii) * ldc + j];
-            }
-            f.dst[(int64_t)i * ldc + j] = v;
         }
     }
 }
@@ -748,8 +747,7 @@ static int run_fold(T *const *src, T *const *dst, const int *probs, int np, cons
         fb.d[q].C = cols[p];
         fb.d[q].by_rows = by_rows;
     }
-    const int64_t tot = (int64_t)N * N;
-    dim3 grid((unsigned)((tot + 255) / 256), 1, np);
+    dim3 grid((unsigned)((N + 255) / 256), (unsigned)N, np);
     k_fold<T><<<grid, 256, 0, st>>>(fb);
     LCB_LAUNCH_CHECK("k_fold");
     return LCB_OK;

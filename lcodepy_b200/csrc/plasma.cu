@@ -22,8 +22,9 @@ k_move_wo_fields(int64_t n, double xi_step, const double *__restrict__ m,
         double xo = xo_p[k], yo = yo_p[k];
         if (mk != 0) {
             const double gm = sqrt(mk * mk + pz * pz + px * px + py * py);
-            xo += px / (gm - pz) * xi_step;
-            yo += py / (gm - pz) * xi_step;
+            const double adv = xi_step / (gm - pz);
+            xo += px * adv;
+            yo += py * adv;
         }
         xo_f[k] = xo; yo_f[k] = yo;
         px_f[k] = px; py_f[k] = py; pz_f[k] = pz;
@@ -94,25 +95,29 @@ k_move_smart(int64_t n, double xi_step, double boundary, double h, int N,
             atomicOr(err, LCB_DEVERR_PLASMA_STENCIL);
         }
         const double mk = m[k];
+        // velocities as p * (1/gamma m): one quotient per pass instead of three
         double gm = sqrt(mk * mk + px * px + py * py + pz * pz);
-        double vx = px / gm, vy = py / gm, vz = pz / gm;
-        double f = qk * xi_step / (1 - pz / gm);
+        double ig = 1.0 / gm;
+        double vx = px * ig, vy = py * ig, vz = pz * ig;
+        double f = qk * xi_step / (1 - vz);
         double dpx = f * (Ex + vy * Bz - vz * By);
         double dpy = f * (Ey - vx * Bz + vz * Bx);
         double dpz = f * (Ez + vx * By - vy * Bx);
-        px = opx + dpx / 2; py = opy + dpy / 2; pz = opz + dpz / 2;
+        px = opx + dpx * 0.5; py = opy + dpy * 0.5; pz = opz + dpz * 0.5;
 
         gm = sqrt(mk * mk + px * px + py * py + pz * pz);
-        vx = px / gm; vy = py / gm; vz = pz / gm;
-        f = qk * xi_step / (1 - pz / gm);
+        ig = 1.0 / gm;
+        vx = px * ig; vy = py * ig; vz = pz * ig;
+        f = qk * xi_step / (1 - vz);
         dpx = f * (Ex + vy * Bz - vz * By);
         dpy = f * (Ey - vx * Bz + vz * Bx);
         dpz = f * (Ez + vx * By - vy * Bx);
-        px = opx + dpx / 2; py = opy + dpy / 2; pz = opz + dpz / 2;
+        px = opx + dpx * 0.5; py = opy + dpy * 0.5; pz = opz + dpz * 0.5;
 
         gm = sqrt(mk * mk + px * px + py * py + pz * pz);
-        double xo = xo_p[k] + px / (gm - pz) * xi_step;
-        double yo = yo_p[k] + py / (gm - pz) * xi_step;
+        const double adv = xi_step / (gm - pz);
+        double xo = xo_p[k] + px * adv;
+        double yo = yo_p[k] + py * adv;
         px = opx + dpx; py = opy + dpy; pz = opz + dpz;
 
         double x = xi0 + xo, y = yi0 + yo;
@@ -167,6 +172,49 @@ __device__ __forceinline__ void tile_slot(int q, bool two_per_cell, int &ti, int
     }
 }
 
+// Deposit one particle's 25-point stencil (weights.py:151-190 arithmetic)
+// into the block's shared window, or straight into HBM when the stencil
+// leaves the window.  dep = false: nothing to deposit.
+template <typename Acc, int WX, int WY>
+__device__ __forceinline__ void deposit_one(Acc *sw, Acc *gro, Acc *gjx, Acc *gjy, Acc *gjz,
+                                            int N, double h, int wx0, int wy0, bool dep,
+                                            int ix, int iy, double xl, double yl,
+                                            double dro, double djx, double djy, double djz)
+{
+    constexpr int WSZ = WX * WY;
+    if (!dep) return;
+    double wx[5], wy[5];
+    weights4(xl, wx);
+    weights4(yl, wy);
+    // w = (wx / h) (wy / h), with 1/h multiplications for the 30 quotients
+    const double ih = 1.0 / h;
+#pragma unroll
+    for (int b = 0; b < 5; b++) wy[b] *= ih;
+    const int lx = ix - 2 - wx0, ly = iy - 2 - wy0;
+    const bool inwin = lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY;
+#pragma unroll
+    for (int a = 0; a < 5; a++) {
+        const double wxa = wx[a] * ih;
+#pragma unroll
+        for (int b = 0; b < 5; b++) {
+            const double w = wxa * wy[b];
+            if (inwin) {
+                const int c = (lx + a) * WY + ly + b;
+                atomicAdd(sw + c, Acc(dro * w));
+                atomicAdd(sw + WSZ + c, Acc(djx * w));
+                atomicAdd(sw + 2 * WSZ + c, Acc(djy * w));
+                atomicAdd(sw + 3 * WSZ + c, Acc(djz * w));
+            } else {
+                const int64_t c = (int64_t)(ix + a - 2) * N + iy + b - 2;
+                atomicAdd(gro + c, Acc(dro * w));
+                atomicAdd(gjx + c, Acc(djx * w));
+                atomicAdd(gjy + c, Acc(djy * w));
+                atomicAdd(gjz + c, Acc(djz * w));
+            }
+        }
+    }
+}
+
 template <typename Acc>
 __global__ void __launch_bounds__(DEP_THREADS)
 k_deposit_tiled(int64_t n_per_sort, int Ns, int N, double h,
@@ -206,54 +254,31 @@ k_deposit_tiled(int64_t n_per_sort, int Ns, int N, double h,
         int ti, tj;
         tile_slot(threadIdx.x + r * DEP_THREADS, two, ti, tj);
         const int i = i0 + ti, j = j0 + tj;
-        if (i >= Ns || j >= Ns) continue;
-        const int64_t k = base + (int64_t)i * Ns + j;
-        const double q = q_a[k];
-        if (q == 0) continue;
-        const double m = m_a[k], px = px_a[k], py = py_a[k], pz = pz_a[k];
-        const double gm = sqrt(m * m + px * px + py * py + pz * pz);
-        const double dro = q / (1 - pz / gm);
-        const double djx = px * (dro / gm), djy = py * (dro / gm), djz = pz * (dro / gm);
-        double xl, yl;
-        const int ix = cell_of((x_init[k] + x_offt[k]) / h + 0.5, half_n, xl);
-        const int iy = cell_of((y_init[k] + y_offt[k]) / h + 0.5, half_n, yl);
-        if (!(ix >= 2 && ix < N - 2 && iy >= 2 && iy < N - 2)) {
-            if (err) atomicOr(err, LCB_DEVERR_PLASMA_STENCIL);
-            continue;
-        }
-        double wx[5], wy[5];
-        weights4(xl, wx);
-        weights4(yl, wy);
-        const int lx = ix - 2 - wx0, ly = iy - 2 - wy0;
-        if (lx >= 0 && lx + 5 <= DEP_WX && ly >= 0 && ly + 5 <= DEP_WY) {
-#pragma unroll
-            for (int a = 0; a < 5; a++) {
-                const double wxa = wx[a] / h;
-#pragma unroll
-                for (int b = 0; b < 5; b++) {
-                    const double w = wxa * wy[b] / h;
-                    const int c = (lx + a) * DEP_WY + ly + b;
-                    atomicAdd(sw + c, Acc(dro * w));
-                    atomicAdd(sw + WSZ + c, Acc(djx * w));
-                    atomicAdd(sw + 2 * WSZ + c, Acc(djy * w));
-                    atomicAdd(sw + 3 * WSZ + c, Acc(djz * w));
-                }
-            }
-        } else {
-#pragma unroll
-            for (int a = 0; a < 5; a++) {
-                const double wxa = wx[a] / h;
-#pragma unroll
-                for (int b = 0; b < 5; b++) {
-                    const double w = wxa * wy[b] / h;
-                    const int64_t c = (int64_t)(ix + a - 2) * N + iy + b - 2;
-                    atomicAdd(gro + c, Acc(dro * w));
-                    atomicAdd(gjx + c, Acc(djx * w));
-                    atomicAdd(gjy + c, Acc(djy * w));
-                    atomicAdd(gjz + c, Acc(djz * w));
+        bool dep = i < Ns && j < Ns;
+        double dro = 0, djx = 0, djy = 0, djz = 0, xl = 0, yl = 0;
+        int ix = 0, iy = 0;
+        if (dep) {
+            const int64_t k = base + (int64_t)i * Ns + j;
+            const double q = q_a[k];
+            if (q == 0) {
+                dep = false;
+            } else {
+                const double m = m_a[k], px = px_a[k], py = py_a[k], pz = pz_a[k];
+                const double gm = sqrt(m * m + px * px + py * py + pz * pz);
+                const double ig = 1.0 / gm;
+                dro = q / (1 - pz * ig);
+                const double rg = dro * ig;
+                djx = px * rg; djy = py * rg; djz = pz * rg;
+                ix = cell_of((x_init[k] + x_offt[k]) / h + 0.5, half_n, xl);
+                iy = cell_of((y_init[k] + y_offt[k]) / h + 0.5, half_n, yl);
+                if (!(ix >= 2 && ix < N - 2 && iy >= 2 && iy < N - 2)) {
+                    if (err) atomicOr(err, LCB_DEVERR_PLASMA_STENCIL);
+                    dep = false;
                 }
             }
         }
+        deposit_one<Acc, DEP_WX, DEP_WY>(sw, gro, gjx, gjy, gjz, N, h, wx0, wy0, dep, ix, iy,
+                                          xl, yl, dro, djx, djy, djz);
     }
     __syncthreads();
     for (int t = threadIdx.x; t < WSZ; t += blockDim.x) {
@@ -272,6 +297,252 @@ template <typename T>
 static size_t deposit_smem_bytes()
 {
     return (size_t)4 * DEP_WX * DEP_WY * sizeof(T);
+}
+
+// ---------------------------------------------------------------------------
+// Fused predictor-corrector stage: K2 (move_smart) followed by K3 (deposit)
+// of the same particles, and for the first stage of an xi step K1 (the
+// free-streaming estimate) in front.  A block owns a lattice tile of TI x TJ
+// particles; the six field planes are staged in a shared-memory window around
+// the tile for the midpoint gather, the new position is deposited into a
+// second window, flushed with global atomics.  Particles whose stencil leaves
+// a window use global memory directly, so the result never depends on the
+// tiling.  Each particle's arithmetic is exactly that of K1, K2 and K3.
+// ---------------------------------------------------------------------------
+template <int WX, int WY>
+struct MdWin {
+    static constexpr int WSZ = WX * WY;
+};
+
+template <typename Acc, int WX, int WY, bool FIRST>
+__global__ void __launch_bounds__(DEP_THREADS)
+k_move_deposit(int64_t n_per_sort, int Ns, int N, double h, double xi_step, double boundary,
+               const double *__restrict__ Exf, const double *__restrict__ Eyf,
+               const double *__restrict__ Ezf, const double *__restrict__ Bxf,
+               const double *__restrict__ Byf, const double *__restrict__ Bzf,
+               const double *__restrict__ x_init, const double *__restrict__ y_init,
+               const double *__restrict__ xo_p, const double *__restrict__ yo_p,
+               const double *__restrict__ px_p, const double *__restrict__ py_p,
+               const double *__restrict__ pz_p, const double *__restrict__ q_p,
+               const double *__restrict__ m_a,
+               double *q_f, double *xo_f, double *yo_f, double *px_f, double *py_f,
+               double *pz_f, Acc *ro, Acc *jx, Acc *jy, Acc *jz, int *err)
+{
+    constexpr int WSZ = WX * WY;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *sf = reinterpret_cast<double *>(smem_raw);          // [6][WX][WY] fields
+    Acc *sw = reinterpret_cast<Acc *>(sf + 6 * WSZ);           // [4][WX][WY] deposit
+    const int s = blockIdx.z;
+    const int i0 = blockIdx.y * DEP_TI, j0 = blockIdx.x * DEP_TJ;
+    const int64_t base = (int64_t)s * n_per_sort;
+    const int half_n = N / 2;
+    const int64_t NN = (int64_t)N * N;
+    Acc *gro = ro + s * NN, *gjx = jx + s * NN, *gjy = jy + s * NN, *gjz = jz + s * NN;
+    const double *fld[6] = {Exf, Eyf, Ezf, Bxf, Byf, Bzf};
+
+    double dummy;
+    const int64_t k0 = base + (int64_t)i0 * Ns + j0;
+    const int wx0 = cell_of(x_init[k0] / h + 0.5, half_n, dummy) - 2 - DEP_SLACK;
+    const int wy0 = cell_of(y_init[k0] / h + 0.5, half_n, dummy) - 2 - DEP_SLACK;
+    bool two = false;
+    if (i0 + 1 < Ns) {
+        const double d = x_init[k0 + Ns] - x_init[k0];
+        two = fabs(2 * d - h) < 0.25 * h;
+    }
+    for (int t = threadIdx.x; t < 4 * WSZ; t += blockDim.x) sw[t] = Acc(0);
+    for (int t = threadIdx.x; t < WSZ; t += blockDim.x) {
+        const int gx = wx0 + t / WY, gy = wy0 + t % WY;
+        const bool in = gx >= 0 && gx < N && gy >= 0 && gy < N;
+        const int64_t g = (int64_t)gx * N + gy;
+#pragma unroll
+        for (int f = 0; f < 6; f++) sf[f * WSZ + t] = in ? __ldg(fld[f] + g) : 0.0;
+    }
+    __syncthreads();
+
+#pragma unroll
+    for (int r = 0; r < DEP_PPT; r++) {
+        int ti, tj;
+        tile_slot(threadIdx.x + r * DEP_THREADS, two, ti, tj);
+        const int i = i0 + ti, j = j0 + tj;
+        bool dep = false;
+        double dro = 0, djx = 0, djy = 0, djz = 0, xl2 = 0, yl2 = 0;
+        int jx2 = 0, jy2 = 0;
+        if (i < Ns && j < Ns) {
+            const int64_t k = base + (int64_t)i * Ns + j;
+            const double mk = m_a[k];
+            const double opx = px_p[k], opy = py_p[k], opz = pz_p[k];
+            const double xo0 = xo_p[k], yo0 = yo_p[k];
+            double qk, xof, yof;
+            if (FIRST) {
+                // K1: full = prev, offsets free-streamed (move.py:292-313)
+                qk = q_p[k];
+                xof = xo0; yof = yo0;
+                if (mk != 0) {
+                    const double gm = sqrt(mk * mk + opz * opz + opx * opx + opy * opy);
+                    const double adv = xi_step / (gm - opz);
+                    xof += opx * adv;
+                    yof += opy * adv;
+                }
+            } else {
+                qk = q_f[k];
+                xof = xo_f[k]; yof = yo_f[k];
+            }
+            if (qk == 0) {
+                // skipped by K2 (and K3): the full state stays as it is
+                if (FIRST) {
+                    xo_f[k] = xof; yo_f[k] = yof;
+                    px_f[k] = opx; py_f[k] = opy; pz_f[k] = opz;
+                    q_f[k] = qk;
+                }
+            } else {
+                // ---- K2 (move.py:169-289) ----
+                const double xi0 = x_init[k], yi0 = y_init[k];
+                double px = opx, py = opy, pz = opz;
+                double xh = xi0 + (xo0 + xof) / 2;
+                double yh = yi0 + (yo0 + yof) / 2;
+                if (xh > boundary)  { xh =  2 * boundary - xh; px = py = pz = 0; }
+                if (xh < -boundary) { xh = -2 * boundary - xh; px = py = pz = 0; }
+                if (yh > boundary)  { yh =  2 * boundary - yh; px = py = pz = 0; }
+                if (yh < -boundary) { yh = -2 * boundary - yh; px = py = pz = 0; }
+                double xl, yl;
+                const int ix = cell_of(xh / h + 0.5, half_n, xl);
+                const int iy = cell_of(yh / h + 0.5, half_n, yl);
+                double Ex = 0, Ey = 0, Ez = 0, Bx = 0, By = 0, Bz = 0;
+                if (ix >= 2 && ix < N - 2 && iy >= 2 && iy < N - 2) {
+                    double wx[5], wy[5];
+                    weights4(xl, wx);
+                    weights4(yl, wy);
+                    const int lx = ix - 2 - wx0, ly = iy - 2 - wy0;
+                    if (lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY) {
+#pragma unroll
+                        for (int a = 0; a < 5; a++) {
+                            const int row = (lx + a) * WY + ly;
+#pragma unroll
+                            for (int b = 0; b < 5; b++) {
+                                const double w = wx[a] * wy[b];
+                                const int c = row + b;
+                                Ex += sf[c] * w; Bx += sf[3 * WSZ + c] * w;
+                                Ey += sf[WSZ + c] * w; By += sf[4 * WSZ + c] * w;
+                                Ez += sf[2 * WSZ + c] * w; Bz += sf[5 * WSZ + c] * w;
+                            }
+                        }
+                    } else {
+#pragma unroll
+                        for (int a = 0; a < 5; a++) {
+                            const int row = (ix + a - 2) * N + iy - 2;
+#pragma unroll
+                            for (int b = 0; b < 5; b++) {
+                                const double w = wx[a] * wy[b];
+                                const int idx = row + b;
+                                Ex += __ldg(Exf + idx) * w; Bx += __ldg(Bxf + idx) * w;
+                                Ey += __ldg(Eyf + idx) * w; By += __ldg(Byf + idx) * w;
+                                Ez += __ldg(Ezf + idx) * w; Bz += __ldg(Bzf + idx) * w;
+                            }
+                        }
+                    }
+                } else if (err) {
+                    atomicOr(err, LCB_DEVERR_PLASMA_STENCIL);
+                }
+                double gm = sqrt(mk * mk + px * px + py * py + pz * pz);
+                double ig = 1.0 / gm;
+                double vx = px * ig, vy = py * ig, vz = pz * ig;
+                double f = qk * xi_step / (1 - vz);
+                double dpx = f * (Ex + vy * Bz - vz * By);
+                double dpy = f * (Ey - vx * Bz + vz * Bx);
+                double dpz = f * (Ez + vx * By - vy * Bx);
+                px = opx + dpx * 0.5; py = opy + dpy * 0.5; pz = opz + dpz * 0.5;
+                gm = sqrt(mk * mk + px * px + py * py + pz * pz);
+                ig = 1.0 / gm;
+                vx = px * ig; vy = py * ig; vz = pz * ig;
+                f = qk * xi_step / (1 - vz);
+                dpx = f * (Ex + vy * Bz - vz * By);
+                dpy = f * (Ey - vx * Bz + vz * Bx);
+                dpz = f * (Ez + vx * By - vy * Bx);
+                px = opx + dpx * 0.5; py = opy + dpy * 0.5; pz = opz + dpz * 0.5;
+                gm = sqrt(mk * mk + px * px + py * py + pz * pz);
+                const double adv = xi_step / (gm - pz);
+                double xo = xo0 + px * adv;
+                double yo = yo0 + py * adv;
+                px = opx + dpx; py = opy + dpy; pz = opz + dpz;
+                double x = xi0 + xo, y = yi0 + yo;
+                if (x > boundary)  { x =  2 * boundary - x; xo = x - xi0; px = py = pz = 0; }
+                if (x < -boundary) { x = -2 * boundary - x; xo = x - xi0; px = py = pz = 0; }
+                if (y > boundary)  { y =  2 * boundary - y; yo = y - yi0; px = py = pz = 0; }
+                if (y < -boundary) { y = -2 * boundary - y; yo = y - yi0; px = py = pz = 0; }
+                bool absorbed = false;
+                if (x >= boundary || x <= -boundary || y >= boundary || y <= -boundary) {
+                    xo = yo = 0; px = py = pz = 0;
+                    absorbed = true;
+                }
+                xo_f[k] = xo; yo_f[k] = yo;
+                px_f[k] = px; py_f[k] = py; pz_f[k] = pz;
+                if (FIRST || absorbed) q_f[k] = absorbed ? 0.0 : qk;
+                if (!absorbed) {
+                    // ---- K3 on the new state (weights.py:151-190) ----
+                    const double gd = sqrt(mk * mk + px * px + py * py + pz * pz);
+                    const double igd = 1.0 / gd;
+                    dro = qk / (1 - pz * igd);
+                    const double rg = dro * igd;
+                    djx = px * rg; djy = py * rg; djz = pz * rg;
+                    jx2 = cell_of((xi0 + xo) / h + 0.5, half_n, xl2);
+                    jy2 = cell_of((yi0 + yo) / h + 0.5, half_n, yl2);
+                    if (jx2 >= 2 && jx2 < N - 2 && jy2 >= 2 && jy2 < N - 2) dep = true;
+                    else if (err) atomicOr(err, LCB_DEVERR_PLASMA_STENCIL);
+                }
+            }
+        }
+        deposit_one<Acc, WX, WY>(sw, gro, gjx, gjy, gjz, N, h, wx0, wy0, dep, jx2, jy2,
+                                  xl2, yl2, dro, djx, djy, djz);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < WSZ; t += blockDim.x) {
+        const int gx = wx0 + t / WY, gy = wy0 + t % WY;
+        if (gx < 0 || gx >= N || gy < 0 || gy >= N) continue;
+        const int64_t c = (int64_t)gx * N + gy;
+        const Acc v0 = sw[t], v1 = sw[WSZ + t], v2 = sw[2 * WSZ + t], v3 = sw[3 * WSZ + t];
+        if (v0 != Acc(0)) atomicAdd(gro + c, v0);
+        if (v1 != Acc(0)) atomicAdd(gjx + c, v1);
+        if (v2 != Acc(0)) atomicAdd(gjy + c, v2);
+        if (v3 != Acc(0)) atomicAdd(gjz + c, v3);
+    }
+}
+
+template <typename Acc, int WX, int WY>
+static size_t move_deposit_smem() { return (size_t)WX * WY * (6 * sizeof(double) + 4 * sizeof(Acc)); }
+
+template <typename Acc, int WX, int WY, bool FIRST>
+static int launch_move_deposit(const lcb_move_deposit_args *a, dim3 grid, Acc *ro, Acc *jx,
+                               Acc *jy, Acc *jz, cudaStream_t st)
+{
+    const size_t sm = move_deposit_smem<Acc, WX, WY>();
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k_move_deposit<Acc, WX, WY, FIRST>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return cuda_check(e, "move_deposit smem attribute");
+        attr = true;
+    }
+    const lcb_plasma_particles &p = a->prev, &f = a->full;
+    k_move_deposit<Acc, WX, WY, FIRST><<<grid, DEP_THREADS, sm, st>>>(
+        a->n_per_sort, a->particles_side, a->grid_steps, a->h, a->xi_step, a->boundary,
+        a->fields[0], a->fields[1], a->fields[2], a->fields[3], a->fields[4], a->fields[5],
+        p.x_init, p.y_init, p.x_offt, p.y_offt, p.px, p.py, p.pz, p.q, p.m,
+        f.q, f.x_offt, f.y_offt, f.px, f.py, f.pz, ro, jx, jy, jz, a->err);
+    return LCB_OK;
+}
+
+template <typename Acc>
+static int dispatch_move_deposit(const lcb_move_deposit_args *a, dim3 grid, Acc *ro, Acc *jx,
+                                 Acc *jy, Acc *jz, cudaStream_t st)
+{
+    // window: the tile's cells (8 x 16 with two or more particles per cell,
+    // 16 x 32 with one) + 2 stencil + 4 slack on each side
+    const bool small = a->lattice_fineness >= 2;
+    if (small)
+        return a->first ? launch_move_deposit<Acc, 20, 28, true>(a, grid, ro, jx, jy, jz, st)
+                        : launch_move_deposit<Acc, 20, 28, false>(a, grid, ro, jx, jy, jz, st);
+    return a->first ? launch_move_deposit<Acc, DEP_WX, DEP_WY, true>(a, grid, ro, jx, jy, jz, st)
+                    : launch_move_deposit<Acc, DEP_WX, DEP_WY, false>(a, grid, ro, jx, jy, jz, st);
 }
 
 __global__ void k_f32_to_f64(int64_t n, const float *__restrict__ a, double *__restrict__ b)
@@ -401,6 +672,56 @@ extern "C" int lcb_plasma_deposit(
     }
     if (ro_initial) {
         cudaError_t e = cudaMemcpyAsync(ro + plane, ro_initial, plane * sizeof(double),
+                                        cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return cuda_check(e, "copy ro_initial");
+    }
+    return LCB_OK;
+}
+
+extern "C" int lcb_plasma_move_deposit(const lcb_move_deposit_args *a, void *stream)
+{
+    LCB_REQUIRE(a, "args is NULL");
+    const int N = a->grid_steps;
+    LCB_REQUIRE(a->n_sorts >= 1 && a->n_sorts <= 2, "n_sorts must be 1 or 2");
+    LCB_REQUIRE((int64_t)a->particles_side * a->particles_side == a->n_per_sort,
+                "n_per_sort (%lld) must be particles_side^2 (%d^2)",
+                (long long)a->n_per_sort, a->particles_side);
+    LCB_REQUIRE(N >= 5, "grid_steps < 5");
+    LCB_REQUIRE(a->precision == LCB_PREC_FP64 || a->precision == LCB_PREC_MIXED, "bad precision");
+    for (int f = 0; f < 6; f++) LCB_REQUIRE(a->fields[f], "field plane %d is NULL", f);
+    cudaStream_t st = as_stream(stream);
+    const size_t plane = (size_t)N * N;
+    for (double *p : {a->ro, a->jx, a->jy, a->jz}) {
+        cudaError_t e = cudaMemsetAsync(p, 0, 2 * plane * sizeof(double), st);
+        if (e != cudaSuccess) return cuda_check(e, "memset currents");
+    }
+    if (a->n_per_sort > 0) {
+        dim3 grid((a->particles_side + DEP_TJ - 1) / DEP_TJ,
+                  (a->particles_side + DEP_TI - 1) / DEP_TI, a->n_sorts);
+        if (a->precision == LCB_PREC_FP64) {
+            const int rc = dispatch_move_deposit<double>(a, grid, a->ro, a->jx, a->jy, a->jz, st);
+            if (rc) return rc;
+            LCB_LAUNCH_CHECK("k_move_deposit<double>");
+        } else {
+            LCB_REQUIRE(a->workspace && a->workspace_bytes >= lcb_plasma_deposit_workspace_bytes(N, a->precision),
+                        "deposit workspace too small");
+            float *w = static_cast<float *>(a->workspace);
+            cudaError_t e = cudaMemsetAsync(w, 0, 8 * plane * sizeof(float), st);
+            if (e != cudaSuccess) return cuda_check(e, "memset f32 currents");
+            const int rc = dispatch_move_deposit<float>(a, grid, w, w + 2 * plane, w + 4 * plane,
+                                                        w + 6 * plane, st);
+            if (rc) return rc;
+            LCB_LAUNCH_CHECK("k_move_deposit<float>");
+            const int64_t cnt = (int64_t)2 * plane;
+            double *outs[4] = {a->ro, a->jx, a->jy, a->jz};
+            for (int qd = 0; qd < 4; qd++) {
+                k_f32_to_f64<<<grid_for(cnt, 256), 256, 0, st>>>(cnt, w + qd * 2 * plane, outs[qd]);
+                LCB_LAUNCH_CHECK("k_f32_to_f64");
+            }
+        }
+    }
+    if (a->ro_initial) {
+        cudaError_t e = cudaMemcpyAsync(a->ro + plane, a->ro_initial, plane * sizeof(double),
                                         cudaMemcpyDeviceToDevice, st);
         if (e != cudaSuccess) return cuda_check(e, "copy ro_initial");
     }

@@ -21,8 +21,8 @@ import torch
 from . import _lib
 from .config import Config
 from .data import Arrays
-from .plasma3d import (CURRENT_NAMES, FIELD_NAMES, FieldOperators, PlasmaState,
-                       host_initial_particles, plasma_params, sorts_of)
+from .plasma3d import (CURRENT_NAMES, FIELD_NAMES, PARTICLE_NAMES, FieldOperators,
+                       PlasmaState, host_initial_particles, plasma_params, sorts_of)
 
 
 class FieldSet:
@@ -96,6 +96,11 @@ class Plane2d3vPlasmaSolver:
         # planes are copied into fixed buffers so the graphs stay valid.
         pe = config.getraw('cuda-graphs')
         self.use_graphs = True if pe is None else bool(pe)
+        # one fused kernel per predictor-corrector stage (move + deposit):
+        # faster with FP32 accumulation; in FP64 the separate kernels win
+        pf = config.getraw('fused-particle-kernels')
+        self.fused = (self.precision == _lib.LCB_PREC_MIXED) if pf is None else bool(pf)
+        self.fineness = max(1, int(round(config.getfloat('plasma-fineness') or 1)))
         self.rbf = torch.zeros(N, N, dtype=torch.float64, device=dev)
         self.rbp = torch.zeros(N, N, dtype=torch.float64, device=dev)
         self.graphs = [None, None]
@@ -189,6 +194,24 @@ class Plane2d3vPlasmaSolver:
             full.px.data_ptr(), full.py.data_ptr(), full.pz.data_ptr(),
             self.err.data_ptr(), _lib.stream_handle()), "lcb_plasma_move_smart")
 
+    def _move_deposit(self, F: FieldSet, prev: PlasmaState, full: PlasmaState,
+                      out: CurrentSet, first: bool):
+        a = _lib.MoveDepositArgs()
+        a.n_per_sort, a.n_sorts, a.particles_side = prev.n_per_sort, self.n_sorts, prev.Ns
+        a.grid_steps, a.precision, a.first = self.N, self.precision, int(first)
+        a.lattice_fineness = self.fineness
+        a.xi_step, a.boundary, a.h = self.dxi, self.boundary, self.h
+        for i in range(6):
+            a.fields[i] = F.buf[i].data_ptr()
+        a.prev = _lib.PlasmaParticles(*(prev.t[k].data_ptr() for k in PARTICLE_NAMES))
+        a.full = _lib.PlasmaParticles(*(full.t[k].data_ptr() for k in PARTICLE_NAMES))
+        a.ro_initial = self.ro_initial.data_ptr() if self.ion_model == "background" else None
+        a.ro, a.jx, a.jy, a.jz = (out.buf[i].data_ptr() for i in range(4))
+        a.workspace, a.workspace_bytes = self.ws_dep.data_ptr(), self.ws_dep.numel()
+        a.err = self.err.data_ptr()
+        _lib.check(_lib.load().lcb_plasma_move_deposit(C.byref(a), _lib.stream_handle()),
+                   "lcb_plasma_move_deposit")
+
     def _compute_fields(self, F: FieldSet, Fprev: FieldSet, cprev: CurrentSet,
                         cfull: CurrentSet, rb_full, rb_prev, rb_div,
                         out_full: FieldSet | None, out_half: FieldSet):
@@ -260,17 +283,26 @@ class Plane2d3vPlasmaSolver:
         cp, cf = self.currents[p], self.currents[f]
         hA, hB = self.half
         T = self._timed
-        T("move_wo_fields", self._move_wo_fields, prev, full)
-        T("move_smart", self._move_smart, Fp, prev, full)
-        T("deposit", self._deposit, full, cf)
+        if self.fused:
+            T("move_deposit", self._move_deposit, Fp, prev, full, cf, True)
+        else:
+            T("move_wo_fields", self._move_wo_fields, prev, full)
+            T("move_smart", self._move_smart, Fp, prev, full)
+            T("deposit", self._deposit, full, cf)
         T("compute_fields", self._compute_fields, Fp, Fp, cp, cf, rb_full, rb_prev,
           rb_div, None, hA)
-        T("move_smart", self._move_smart, hA, prev, full)
-        T("deposit", self._deposit, full, cf)
+        if self.fused:
+            T("move_deposit", self._move_deposit, hA, prev, full, cf, False)
+        else:
+            T("move_smart", self._move_smart, hA, prev, full)
+            T("deposit", self._deposit, full, cf)
         T("compute_fields", self._compute_fields, hA, Fp, cp, cf, rb_full, rb_prev,
           rb_div, Ff, hB)
-        T("move_smart", self._move_smart, hB, prev, full)
-        T("deposit", self._deposit, full, cf)
+        if self.fused:
+            T("move_deposit", self._move_deposit, hB, prev, full, cf, False)
+        else:
+            T("move_smart", self._move_smart, hB, prev, full)
+            T("deposit", self._deposit, full, cf)
         if advance:
             self.cur = f
             self.last_fields = Fp

@@ -158,3 +158,20 @@ def test_cuda_graphs_match_eager(rigid):
     assert rel_err(ez1, ez0) < 1e-12
     for k in ("Ex", "Ey", "Ez", "Bx", "By", "Bz", "Phi"):
         assert rel_err(getattr(f1, k).cpu().numpy(), getattr(f0, k).cpu().numpy()) < 1e-12, k
+
+
+@pytest.mark.parametrize("extra", [{'rigid-beam': True},
+                                   {'rigid-beam': True, 'ion-model': 'mobile'},
+                                   {'rigid-beam': True, 'plasma-particles-per-cell': 1},
+                                   {'rigid-beam': True, 'precision': 'mixed'}])
+def test_fused_stage_matches_separate_kernels(extra):
+    """The fused move+deposit stage equals K1 + K2 + K3 launched separately."""
+    _, p0, f0, c0, ez0 = run(cfg(**extra, **{'fused-particle-kernels': False}), rigid_driver)
+    _, p1, f1, c1, ez1 = run(cfg(**extra, **{'fused-particle-kernels': True}), rigid_driver)
+    tol = 1e-5 if extra.get('precision') == 'mixed' else 1e-12
+    assert rel_err(ez1, ez0) < tol
+    for k in ("Ex", "Ez", "Bz"):
+        assert rel_err(getattr(f1, k).cpu().numpy(), getattr(f0, k).cpu().numpy()) < tol, k
+    for s in p0:
+        for k in ("x_offt", "px", "q"):
+            assert rel_err(getattr(p1[s], k).cpu().numpy(), getattr(p0[s], k).cpu().numpy()) < tol
