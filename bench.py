@@ -23,6 +23,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -31,6 +32,8 @@ import time
 
 import numpy as np
 
+# many member streams run concurrently in the batch and serve workloads
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -273,6 +276,184 @@ def run_rigid129(args, ws, rank, local):
             "n_iter": n_iter}
 
 
+def run_batch(args, ws, rank, local):
+    """The batched parameter scan: 64 simulations (grids 129, 257, 513 at step
+    0.05, 2 x 2 per cell, rigid Gaussian drivers with seeded amplitudes and
+    widths), advanced together in mixed precision, one xi step per member per
+    bench step on concurrent streams with captured graphs.  The same members
+    are then run one after another through the plain FP64 drop-in path
+    (Simulation with its default settings) for the plain-path comparison and
+    the on-axis Ez error."""
+    import torch
+    from lcodepy_b200 import Simulation
+    from lcodepy_b200.batch import BatchRunner, Member, scan_members
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    W, K = args.warmup, args.steps
+    specs = scan_members(n=args.members, n_steps=W + K, precision=args.precision)
+    members = [Member(c, d, dev) for c, d in specs]
+    runner = BatchRunner(members)
+    for _ in range(W):
+        runner.step()
+    torch.cuda.synchronize()
+    barrier(ws)
+    clock = ClockSampler(local) if rank == 0 else None
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    # all member streams join the current stream around the timed region
+    from lcodepy_b200 import _lib
+    n0 = _lib.launch_count()
+    cur = torch.cuda.current_stream()
+    t0.record(cur)
+    for m in members:
+        m.stream.wait_stream(cur)
+    for _ in range(K):
+        runner.step()
+    for m in members:
+        cur.wait_stream(m.stream)
+    t1.record(cur)
+    torch.cuda.synchronize()
+    launches = _lib.launch_count() - n0
+    clocks = clock.stop() if clock else None
+    ms = max_over_ranks(t0.elapsed_time(t1), ws)
+    cells = sum(m.cells for m in members)
+    value = ws * cells * K / (ms / 1e3)
+    ez_batch = [m.result()["ez"] for m in members]
+    for m in members:
+        m.release()
+    del members, runner
+    torch.cuda.empty_cache()
+
+    # plain FP64: each member alone, eager, no graphs, separate kernels
+    plain_ms, errs = 0.0, []
+    for (cfg, drv), ezb in zip(specs, ez_batch):
+        c = {**cfg, 'precision': 'fp64'}
+        sim = Simulation(config=c, beam_parameters=drv, runas_filename='')
+        ps = sim.push_solver
+        ev = {}
+
+        def hook(k, ev=ev):
+            if k == W:
+                ev["a"] = torch.cuda.Event(enable_timing=True)
+                ev["a"].record()
+            if k == W + K:
+                ev["b"] = torch.cuda.Event(enable_timing=True)
+                ev["b"].record()
+        ps.plasma_solver.init_state(1.0)
+        from lcodepy_b200.beam3d import RigidBeamSource
+        ps.step_dt(cfg['xi-step'], RigidBeamSource(None, drv), None, 1.0, [], step_hook=hook)
+        torch.cuda.synchronize()
+        plain_ms += ev["a"].elapsed_time(ev["b"])
+        ez64 = ps.ez_axis.cpu().numpy()
+        errs.append(float(np.linalg.norm(ezb - ez64) / max(np.linalg.norm(ez64), 1e-300)))
+        del sim, ps
+    plain = cells * K / (plain_ms / 1e3)
+    return {"value": value, "ms_per_step": ms / K, "plain": plain, "ratio": value / plain,
+            "ez_err_max": max(errs), "ez_err_median": float(np.median(errs)),
+            "clocks": clocks, "cells": cells, "members": len(specs), "launches": launches}
+
+
+def plain_ms_per_step(N, precision="fp64", n_steps=120, skip=20):
+    """Device ms per xi step of the plain drop-in path (Simulation, default
+    settings) on an N x N rigid-driver grid at h = dxi = 0.05."""
+    import torch
+    from lcodepy_b200 import Simulation
+    from lcodepy_b200.batch import GaussianDriver, request_stream
+    cfg = dict(request_stream(n=1, sizes=(N,), min_steps=n_steps, max_steps=n_steps)[0][2])
+    cfg['precision'] = precision
+    sim = Simulation(config=cfg, beam_parameters=GaussianDriver(), runas_filename='')
+    ps = sim.push_solver
+    ev = {}
+
+    def hook(k):
+        if k in (skip, n_steps):
+            ev[k] = torch.cuda.Event(enable_timing=True)
+            ev[k].record()
+    from lcodepy_b200.beam3d import RigidBeamSource
+    ps.plasma_solver.init_state(1.0)
+    ps.step_dt(cfg['xi-step'], RigidBeamSource(None, GaussianDriver()), None, 1.0, [],
+               step_hook=hook)
+    torch.cuda.synchronize()
+    return ev[skip].elapsed_time(ev[n_steps]) / (n_steps - skip)
+
+
+def run_serve(args, ws, rank, local):
+    """The served stream: requests with Poisson arrivals (20 per second,
+    seeded), grids 129/257/513 at h = 0.05, xi lengths uniform in 200..2000
+    steps of 0.05, rigid Gaussian drivers; admitted by HBM footprint into at
+    most --slots concurrent members, each advanced by captured graphs on its
+    own stream.  The plain comparison runs the same requests one by one, first
+    come first served, through the plain FP64 drop-in path; its per-step cost
+    per grid size is measured here and its schedule computed from the
+    arrivals."""
+    import torch
+    from lcodepy_b200 import _lib
+    from lcodepy_b200.batch import Server, request_stream
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    reqs = request_stream(n=args.requests, precision=args.precision)
+    # warm the library, the allocator and the graph path on a short request
+    warm = Server(hbm_budget_bytes=args.hbm_budget_gb << 30, max_slots=args.slots, device=dev)
+    for N in (129, 257, 513):
+        c = dict(request_stream(n=1, sizes=(N,), min_steps=8, max_steps=8,
+                                precision=args.precision)[0][2])
+        warm.submit(f"warm{N}", c, reqs[0][3], arrival=0.0)
+    warm.run()
+    torch.cuda.synchronize()
+    barrier(ws)
+    srv = Server(hbm_budget_bytes=args.hbm_budget_gb << 30, max_slots=args.slots, device=dev)
+    for arr, rid, cfg, drv in reqs:
+        srv.submit(rid, cfg, drv, arrival=arr)
+    clock = ClockSampler(local) if rank == 0 else None
+    n0 = _lib.launch_count()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    srv.t0 = time.perf_counter()
+    t0.record()
+    srv.run()
+    torch.cuda.synchronize()
+    t1.record()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - srv.t0
+    clocks = clock.stop() if clock else None
+    launches = _lib.launch_count() - n0
+    ms = max_over_ranks(t0.elapsed_time(t1), ws)
+    done = srv.done
+    cell_steps = sum(d["cells"] * d["steps"] for d in done.values())
+    lat = np.array([done[r]["latency"] for _, r, _, _ in reqs])
+    value = ws * cell_steps / (ms / 1e3)
+    # plain path, request by request, first come first served
+    per = {N: plain_ms_per_step(N) for N in (129, 257, 513)}
+    finish, plain_lat, busy = 0.0, [], 0.0
+    for arr, rid, cfg, drv in reqs:
+        d = done[rid]
+        N = int(round(math.sqrt(d["cells"])))
+        dur = d["steps"] * per[N] / 1e3
+        finish = max(finish, arr) + dur
+        busy += dur
+        plain_lat.append(finish - arr)
+    plain_lat = np.array(plain_lat)
+    plain_value = cell_steps / finish
+    # accuracy: a few requests rerun alone through the plain FP64 path
+    errs = []
+    if args.check_requests:
+        from lcodepy_b200 import Simulation
+        for arr, rid, cfg, drv in sorted(reqs, key=lambda r: r[2]['window-length'])[
+                :args.check_requests]:
+            sim = Simulation(config={**cfg, 'precision': 'fp64'}, beam_parameters=drv,
+                             runas_filename='')
+            sim.step()
+            ez64 = sim.push_solver.ez_axis.cpu().numpy()
+            errs.append(float(np.linalg.norm(done[rid]["ez"] - ez64) / np.linalg.norm(ez64)))
+            del sim
+    return {"value": value, "ms": ms, "wall_s": wall, "cell_steps": cell_steps,
+            "p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+            "plain_value": plain_value, "plain_p50": float(np.percentile(plain_lat, 50)),
+            "plain_p99": float(np.percentile(plain_lat, 99)), "plain_ms_per_step": per,
+            "errs": errs, "clocks": clocks, "launches": launches,
+            "span_arrivals_s": reqs[-1][0]}
+
+
 def run_e2e(cfg, beam_host, dev):
     """Simulation.step() from a host beam file to host results: the H2D copy of
     the beam and of the initial plasma and the D2H read of fields, on-axis Ez
@@ -328,7 +509,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--workload", default="production", choices=["production", "rigid129"],
+    ap.add_argument("--members", type=int, default=64, help="batch: scan members")
+    ap.add_argument("--requests", type=int, default=64, help="serve: requests in the stream")
+    ap.add_argument("--slots", type=int, default=32, help="serve: concurrent members")
+    ap.add_argument("--hbm-budget-gb", type=int, default=64, help="serve: HBM admission budget")
+    ap.add_argument("--check-requests", type=int, default=3,
+                    help="serve: requests rerun alone in FP64 for the Ez error")
+    ap.add_argument("--workload", default="production",
+                    choices=["production", "rigid129", "batch", "serve"],
                     help="production: the N=513 FP64 drop-in run (default); rigid129: "
                          "the 129 x 129 rigid-driver configuration")
     ap.add_argument("--cpu-sample", type=int, default=8,
@@ -366,6 +554,49 @@ def main():
             dist.destroy_process_group()
         return
 
+    if args.workload == "batch":
+        r = run_batch(args, ws, rank, local)
+        if rank == 0:
+            print(json.dumps({
+                "metric": METRIC, "value": r["value"], "unit": METRIC, "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "mixed" if args.precision == "mixed" else "f64",
+                "data": "synthetic (seeded rigid Gaussian drivers)",
+                "config": {"workload": f"batched scan: {r['members']} members, grids "
+                                       "129/257/513 at h=0.05, dxi=0.05, ppc=4",
+                           "precision": args.precision,
+                           "steps_are": "batched xi steps (every member advances one)"},
+                "plain_fp64_value": r["plain"], "batched_vs_plain": r["ratio"],
+                "ez_rel_l2_vs_fp64": {"max": r["ez_err_max"], "median": r["ez_err_median"]},
+                "gpu_launches": r["launches"], "clocks": r["clocks"]}), flush=True)
+        return
+    if args.workload == "serve":
+        r = run_serve(args, ws, rank, local)
+        if rank == 0:
+            print(json.dumps({
+                "metric": METRIC, "value": r["value"], "unit": METRIC, "n_gpus": ws,
+                "steps": args.requests, "warmup": args.warmup,
+                "ms_per_step": r["ms"] / args.requests,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "mixed" if args.precision == "mixed" else "f64",
+                "data": "synthetic (seeded Poisson request stream, rigid Gaussian drivers)",
+                "config": {"workload": f"served stream: {args.requests} requests, Poisson "
+                                       "20/s, grids 129/257/513 at h=0.05, 200-2000 xi "
+                                       "steps of 0.05, ppc=4",
+                           "precision": args.precision, "slots": args.slots,
+                           "hbm_budget_gb": args.hbm_budget_gb,
+                           "steps_are": "requests; ms_per_step = makespan / requests",
+                           "l2": "aggregate member state larger than L2"},
+                "latency_s": {"p50": r["p50"], "p99": r["p99"]},
+                "makespan_s": r["ms"] / 1e3, "cell_steps": r["cell_steps"],
+                "plain_fp64": {"value": r["plain_value"], "p50": r["plain_p50"],
+                               "p99": r["plain_p99"],
+                               "ms_per_step": r["plain_ms_per_step"]},
+                "served_vs_plain": r["value"] / r["plain_value"],
+                "ez_rel_l2_vs_fp64": r["errs"],
+                "gpu_launches": r["launches"], "clocks": r["clocks"]}), flush=True)
+        return
     if args.workload == "rigid129":
         r = run_rigid129(args, ws, rank, local)
         if rank == 0:

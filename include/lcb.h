@@ -288,6 +288,29 @@ typedef struct lcb_beam_step_args {
  * move_beam_layer, create_next_layer, push_beam_layer). */
 int lcb_beam_step(const lcb_beam_step_args *a, void *stream);
 
+/* ---------------------------------------------------------------------
+ * Capturable xi steps (batched and served simulations)
+ * ------------------------------------------------------------------- */
+
+/* Rigid Gaussian driver of the benchmark configurations evaluated on the
+ * device for xi step first_layer + *counter (device int64):
+ *   rho = amplitude exp(-r^2 / (2 sigma_r^2)) (1 + cos(sqrt(pi/2) xi)) / 2
+ * for -xi_len <= xi <= 0, else 0, on the reference's meshgrid
+ * (beam_calculator.py:158-170); rho_prev is the previous step's plane (zeros
+ * for the first).  Replaces the per-step host call of the driver function in
+ * RigidBeamCalculator.layout_beam_layer (beam_calculator.py:166-170) for this
+ * family of drivers, so a captured graph needs no host input. */
+int lcb_rigid_gaussian(int grid_steps, double h, double xi_step, double amplitude,
+                       double sigma_r, double xi_len, int64_t first_layer,
+                       const int64_t *counter, double *rho_full, double *rho_prev,
+                       void *stream);
+
+/* history[*counter] = plane[N/2][N/2] (the on-axis value), then *counter += 1.
+ * The device-side form of the per-step on-axis Ez record
+ * (push_solver.py:541-547). */
+int lcb_record_axis(const double *plane, int grid_steps, int64_t *counter,
+                    double *history, int64_t capacity, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -100,6 +100,8 @@ _SIGS = {
     "lcb_beam_deposit": (_i, [_i64, _i, _d, _d, _i64] + [_vp] * 6 + [_vp, _vp]),
     "lcb_beam_substepping": (_i, [_i64, _vp, _vp, _d, _d, _vp, _vp, _vp]),
     "lcb_beam_step": (_i, [C.POINTER(BeamStepArgs), _vp]),
+    "lcb_rigid_gaussian": (_i, [_i, _d, _d, _d, _d, _d, _i64, _vp, _vp, _vp, _vp]),
+    "lcb_record_axis": (_i, [_vp, _i, _vp, _vp, _i64, _vp]),
     "lcb_beam_move": (_i, [_i64, _d, _d, _i64, _d, _i, _vp, _vp,
                            C.POINTER(Fields7), C.POINTER(Fields7)] + [_vp] * 9 + [_vp, _vp]),
 }

@@ -1,0 +1,329 @@
+"""Many simulations on one GPU: batched parameter scans and a served request
+stream.
+
+Each ``Member`` is one quasistatic 3D simulation with a rigid Gaussian driver
+(the driver family of the benchmark configurations).  Its whole xi step --
+driver evaluated on the device from a step counter, predictor-corrector
+plasma step, on-axis Ez record -- is captured once in two CUDA graphs (one
+per parity of the rotating buffers) and replayed on the member's own stream,
+so members of any grid size advance concurrently and a host loop only issues
+one graph launch per member and xi step.
+
+``BatchRunner`` advances a fixed set of members together (a parameter scan).
+``Server`` admits requests that arrive over time into free slots while others
+run (continuous batching), bounded by an HBM budget, and reports each
+request's completion latency.
+"""
+from __future__ import annotations
+
+import collections
+import dataclasses
+import math
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+from .config import Config
+from .solver import Plane2d3vPlasmaSolver
+
+XI_LEN = math.sqrt(2 * math.pi)
+
+
+@dataclasses.dataclass
+class GaussianDriver:
+    """rho_b = amplitude exp(-r^2 / (2 sigma_r^2)) (1 + cos(sqrt(pi/2) xi)) / 2
+    on -xi_len <= xi <= 0.  Callable with the reference's rigid-beam
+    signature fn(xp, xi, x_grid, y_grid) as well."""
+    amplitude: float = 0.1
+    sigma_r: float = 1.0
+    xi_len: float = XI_LEN
+
+    def __call__(self, xp, xi, x, y):
+        if -self.xi_len <= xi <= 0:
+            return (self.amplitude * xp.exp(-(x ** 2 + y ** 2) / (2 * self.sigma_r ** 2))
+                    * (1 + np.cos(np.sqrt(np.pi / 2) * xi)) / 2)
+        return xp.zeros_like(x)
+
+
+def footprint_bytes(config: dict) -> int:
+    """Device memory one member needs (particles, fields, currents, solver
+    workspaces), for admission decisions."""
+    cfg = Config(config)
+    cfg._adjust_config_values_3d()
+    N = cfg.getint('window-width-steps')
+    f = max(1, int(round(cfg.getfloat('plasma-fineness') or 1)))
+    Ns = (N - 2 * cfg.getint('plasma-padding-steps')) * f
+    sorts = 2 if cfg.get('ion-model') == 'mobile' else 1
+    mixed = str(cfg.getraw('precision') or 'fp64').lower() == 'mixed'
+    L = _lib.load()
+    prec = _lib.LCB_PREC_MIXED if mixed else _lib.LCB_PREC_FP64
+    particles = 2 * 9 * 8 * sorts * Ns * Ns
+    planes = (4 * 7 + 2 * 4 * 2 + 4) * 8 * N * N
+    return int(particles + planes + L.lcb_compute_fields_workspace_bytes(N, prec)
+               + L.lcb_field_operators_bytes(N, prec)
+               + L.lcb_plasma_deposit_workspace_bytes(N, prec) + (8 << 20))
+
+
+class Member:
+    """One simulation whose xi step is a pair of captured CUDA graphs."""
+
+    def __init__(self, config: dict, driver: GaussianDriver, device=None, name=None):
+        self.device = device or torch.device("cuda", torch.cuda.current_device())
+        cfg = Config({**config, 'cuda-graphs': False})
+        cfg._adjust_config_values_3d()
+        self.config = cfg
+        self.name = name
+        self.driver = driver
+        self.N = cfg.getint('window-width-steps')
+        self.h = cfg.getfloat('transverse-step')
+        self.dxi = cfg.getfloat('xi-step')
+        self.n_steps = round(cfg.getfloat('window-length') / self.dxi) + 1
+        self.cells = self.N * self.N
+        self.stream = torch.cuda.Stream(self.device)
+        with torch.cuda.stream(self.stream):
+            self.solver = Plane2d3vPlasmaSolver(cfg, self.device)
+            self.solver.init_state(cfg.getfloat('time-step'))
+            self.counter = torch.zeros(1, dtype=torch.int64, device=self.device)
+            self.ez = torch.zeros(self.n_steps, dtype=torch.float64, device=self.device)
+        self.graphs = [None, None]
+        self.eager = 0
+        self.done = 0
+        self.marks = collections.deque()
+        self.end_event = None
+        self.t_admit = self.t_done = None
+
+    @property
+    def finished(self) -> bool:
+        return self.done >= self.n_steps
+
+    def _ops(self):
+        L = _lib.load()
+        ps = self.solver
+        st = _lib.stream_handle()
+        d = self.driver
+        _lib.check(L.lcb_rigid_gaussian(self.N, self.h, self.dxi, d.amplitude, d.sigma_r,
+                                        d.xi_len, 0, self.counter.data_ptr(),
+                                        ps.rbf.data_ptr(), ps.rbp.data_ptr(), st),
+                   "lcb_rigid_gaussian")
+        ps._step_ops(ps.rbf, ps.rbp, 1.0, advance=False)
+        new = ps.fields[1 - ps.cur]
+        _lib.check(L.lcb_record_axis(new.Ez.data_ptr(), self.N, self.counter.data_ptr(),
+                                     self.ez.data_ptr(), self.n_steps, st), "lcb_record_axis")
+
+    MARK_EVERY = 16
+    MAX_AHEAD = 4
+
+    def step(self):
+        """Issue one xi step on the member's stream (asynchronous).  The host
+        stays at most MARK_EVERY * MAX_AHEAD steps ahead of the device."""
+        ps = self.solver
+        p = ps.cur
+        if len(self.marks) >= self.MAX_AHEAD:
+            self.marks.popleft().synchronize()
+        with torch.cuda.stream(self.stream):
+            if self.eager < 2:
+                self._ops()
+                self.eager += 1
+            else:
+                if self.graphs[p] is None:
+                    # capture on the member's own stream without the
+                    # device-wide synchronisation torch.cuda.graph performs,
+                    # so other members keep running meanwhile
+                    g = torch.cuda.CUDAGraph()
+                    n0 = _lib.load().lcb_launch_count()
+                    g.capture_begin(capture_error_mode="thread_local")
+                    try:
+                        self._ops()
+                    finally:
+                        g.capture_end()
+                    self.graphs[p] = (g, _lib.load().lcb_launch_count() - n0)
+                g, nl = self.graphs[p]
+                g.replay()
+                _lib.add_replayed(nl)
+            self.done += 1
+            if self.done % self.MARK_EVERY == 0 or self.done >= self.n_steps:
+                ev = torch.cuda.Event()
+                ev.record(self.stream)
+                self.marks.append(ev)
+                if self.done >= self.n_steps:
+                    self.end_event = ev
+        ps.cur = 1 - p
+        ps.last_fields = ps.fields[p]
+
+    def complete(self) -> bool:
+        """All steps issued and executed."""
+        return self.end_event is not None and self.end_event.query()
+
+    def result(self):
+        """On-axis Ez per xi step and the final fields (host arrays)."""
+        self.stream.synchronize()
+        return {"ez": self.ez.cpu().numpy(),
+                "fields": self.solver.prev_fields.buf.cpu().numpy()}
+
+    def release(self):
+        self.graphs = [None, None]
+        self.solver = None
+        self.marks.clear()
+
+
+class BatchRunner:
+    """Advance a fixed set of members together, one xi step at a time."""
+
+    def __init__(self, members):
+        self.members = list(members)
+
+    def step(self):
+        for m in self.members:
+            if not m.finished:
+                m.step()
+
+    def run(self, steps=None):
+        n = steps if steps is not None else max(m.n_steps for m in self.members)
+        for _ in range(n):
+            self.step()
+        torch.cuda.synchronize()
+
+    @property
+    def cell_steps_per_step(self):
+        return sum(m.cells for m in self.members if not m.finished)
+
+
+def request_stream(n=500, rate=20.0, seed=4321, dxi=0.05, h=0.05, sizes=(129, 257, 513),
+                   min_steps=200, max_steps=2000, precision="mixed"):
+    """The served stream: n requests with Poisson arrivals of the given mean
+    rate (exponential gaps), grid drawn from sizes, xi length uniform in
+    [min_steps, max_steps] steps of dxi, and a rigid Gaussian driver with
+    amplitude ~ U[0.01, 0.5] and sigma_r ~ U[0.5, 2]; all drawn from
+    numpy.random.default_rng(seed).  Returns (arrival, id, config, driver)."""
+    widths = {129: 3.25, 257: 6.45, 513: 12.85}
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for r in range(n):
+        t += float(rng.exponential(1.0 / rate))
+        N = int(sizes[rng.integers(len(sizes))])
+        steps = int(rng.integers(min_steps, max_steps + 1))
+        drv = GaussianDriver(amplitude=float(rng.uniform(0.01, 0.5)),
+                             sigma_r=float(rng.uniform(0.5, 2.0)))
+        cfg = {'geometry': '3d', 'window-width': widths.get(N, N * h / 2), 'transverse-step': h,
+               'window-length': (steps - 1) * dxi, 'xi-step': dxi,
+               'ion-model': 'background', 'plasma-particles-per-cell': 4,
+               'rigid-beam': True, 'print-every': 0, 'precision': precision,
+               'time-step': 1.0}
+        out.append((t, f"req{r:04d}", cfg, drv))
+    return out
+
+
+def scan_members(n=64, seed=1234, n_steps=1000, precision="mixed", dxi=0.05, h=0.05,
+                 sizes=(129, 257, 513), device=None):
+    """The batched parameter scan: member m has grid sizes[m % 3] at step h,
+    2 x 2 particles per cell, background ions, xi step dxi for n_steps steps,
+    and a rigid Gaussian driver with amplitude ~ U[0.01, 0.5] and sigma_r ~
+    U[0.5, 2] drawn from numpy.random.default_rng(seed + m)."""
+    widths = {129: 3.25, 257: 6.45, 513: 12.85}
+    out = []
+    for m in range(n):
+        rng = np.random.default_rng(seed + m)
+        N = sizes[m % len(sizes)]
+        drv = GaussianDriver(amplitude=float(rng.uniform(0.01, 0.5)),
+                             sigma_r=float(rng.uniform(0.5, 2.0)))
+        cfg = {'geometry': '3d', 'window-width': widths.get(N, N * h / 2), 'transverse-step': h,
+               'window-length': (n_steps - 1) * dxi, 'xi-step': dxi,
+               'ion-model': 'background', 'plasma-particles-per-cell': 4,
+               'rigid-beam': True, 'print-every': 0, 'precision': precision,
+               'time-step': 1.0}
+        out.append((cfg, drv))
+    return out
+
+
+class Server:
+    """Continuous batching of simulation requests on one GPU.
+
+    Requests arrive over time; ``poll`` admits waiting requests (in arrival
+    order) into free slots when their HBM footprint fits the budget, every
+    ``tick`` advances each running request by one xi step (one graph launch on
+    its own stream), and ``retire`` collects requests whose last step has
+    executed, releasing their memory so that waiting ones are admitted while
+    others are still running.  Latency is measured from a request's arrival
+    to the moment its completion is observed."""
+
+    def __init__(self, hbm_budget_bytes: int, max_slots: int = 64, device=None):
+        self.device = device or torch.device("cuda", torch.cuda.current_device())
+        self.budget = hbm_budget_bytes
+        self.max_slots = max_slots
+        self.waiting = collections.deque()   # (arrival, request_id, config, driver)
+        self.running = []                    # (request_id, Member, footprint)
+        self.draining = []                   # all steps issued, not yet complete
+        self.done = {}
+        self.used = 0
+        self.t0 = time.perf_counter()
+
+    def now(self):
+        return time.perf_counter() - self.t0
+
+    def submit(self, request_id, config, driver, arrival=None):
+        item = (self.now() if arrival is None else arrival, request_id, config, driver)
+        if self.waiting and item[0] < self.waiting[-1][0]:
+            w = sorted([*self.waiting, item], key=lambda r: r[0])
+            self.waiting = collections.deque(w)
+        else:
+            self.waiting.append(item)
+
+    def poll(self):
+        """Admit arrived requests, first come first served, while a slot is
+        free and the footprint fits; a request that does not fit waits (and so
+        do the ones behind it, so large requests are not starved)."""
+        t = self.now()
+        while self.waiting:
+            arr, rid, cfg, drv = self.waiting[0]
+            if arr > t or len(self.running) + len(self.draining) >= self.max_slots:
+                break
+            fp = footprint_bytes(cfg)
+            if self.used + fp > self.budget and (self.running or self.draining):
+                break
+            self.waiting.popleft()
+            m = Member(cfg, drv, self.device, name=rid)
+            m.t_arrival = arr
+            m.t_admit = t
+            m.footprint = fp
+            self.running.append(m)
+            self.used += fp
+
+    def tick(self):
+        """One xi step for every running request."""
+        keep = []
+        for m in self.running:
+            m.step()
+            (self.draining if m.finished else keep).append(m)
+        self.running = keep
+
+    def retire(self):
+        keep = []
+        for m in self.draining:
+            if m.complete():
+                t = self.now()
+                self.done[m.name] = {"ez": m.ez.cpu().numpy(), "latency": t - m.t_arrival,
+                                     "arrival": m.t_arrival, "admitted": m.t_admit,
+                                     "finished": t, "cells": m.cells, "steps": m.n_steps}
+                m.release()
+                self.used -= m.footprint
+            else:
+                keep.append(m)
+        self.draining = keep
+
+    def idle(self):
+        return not self.running and not self.draining and not self.waiting
+
+    def run(self):
+        """Serve until every submitted request is done."""
+        while not self.idle():
+            self.poll()
+            if self.running:
+                self.tick()
+            elif self.draining:
+                self.draining[0].end_event.synchronize()
+            elif self.waiting:
+                time.sleep(max(0.0, min(self.waiting[0][0] - self.now(), 0.01)))
+            self.retire()

@@ -56,6 +56,8 @@ default_config_values = {
 # keys, so adding them keeps configs interchangeable).
 #   'precision': 'fp64' (default; the reference's arithmetic) or 'mixed'
 #                (FP32 deposition and FP32 transforms, FP64 particles).
+#   'deposit-precision', 'field-precision': 'fp64' or 'fp32', overriding
+#                'precision' for the deposition or the field solve alone.
 #   'print-every': xi steps between the on-axis Ez lines (reference: 10).
 
 

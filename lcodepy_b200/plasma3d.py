@@ -175,9 +175,23 @@ def plasma_params(config: Config):
         boundary=h * (N / 2 - bp),
         sub_coeff=config.getfloat('field-solver-subtraction-coefficient'),
         ion_model=config.get('ion-model'),
-        precision=_lib.LCB_PREC_MIXED if config.get('precision', 'fp64').lower() == 'mixed'
-        else _lib.LCB_PREC_FP64,
+        precision=_part_precision(config, 'field-precision'),
+        deposit_precision=_part_precision(config, 'deposit-precision'),
     )
+
+
+def _part_precision(config: Config, key: str) -> int:
+    """'precision' sets both parts ('fp64' or 'mixed'); 'field-precision' and
+    'deposit-precision' ('fp64' or 'fp32') override one part each."""
+    v = config.getraw(key)
+    if v is None:
+        mixed = str(config.getraw('precision') or 'fp64').lower() == 'mixed'
+    else:
+        v = str(v).lower()
+        if v not in ('fp64', 'fp32'):
+            raise ValueError(f"{key} must be 'fp64' or 'fp32', not {v!r}")
+        mixed = v == 'fp32'
+    return _lib.LCB_PREC_MIXED if mixed else _lib.LCB_PREC_FP64
 
 
 def host_initial_particles(config: Config, current_time=0.0):

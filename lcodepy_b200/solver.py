@@ -71,6 +71,7 @@ class Plane2d3vPlasmaSolver:
         self.N, self.h, self.dxi = p["N"], p["h"], p["dxi"]
         self.boundary, self.sub_coeff = p["boundary"], p["sub_coeff"]
         self.ion_model, self.precision = p["ion_model"], p["precision"]
+        self.dep_precision = p["deposit_precision"]
         self.sort_names = sorts_of(self.ion_model)
         self.n_sorts = len(self.sort_names)
         _lib.load()
@@ -83,7 +84,7 @@ class Plane2d3vPlasmaSolver:
         self.ws_fields = torch.empty(
             _lib.load().lcb_compute_fields_workspace_bytes(N, self.precision),
             dtype=torch.uint8, device=dev)
-        ws_dep = _lib.load().lcb_plasma_deposit_workspace_bytes(N, self.precision)
+        ws_dep = _lib.load().lcb_plasma_deposit_workspace_bytes(N, self.dep_precision)
         self.ws_dep = torch.empty(max(ws_dep, 256), dtype=torch.uint8, device=dev)
         self.err = torch.zeros(1, dtype=torch.int32, device=dev)
         self.ro_initial = torch.zeros(N, N, dtype=torch.float64, device=dev)
@@ -99,7 +100,7 @@ class Plane2d3vPlasmaSolver:
         # one fused kernel per predictor-corrector stage (move + deposit):
         # faster with FP32 accumulation; in FP64 the separate kernels win
         pf = config.getraw('fused-particle-kernels')
-        self.fused = (self.precision == _lib.LCB_PREC_MIXED) if pf is None else bool(pf)
+        self.fused = (self.dep_precision == _lib.LCB_PREC_MIXED) if pf is None else bool(pf)
         self.fineness = max(1, int(round(config.getfloat('plasma-fineness') or 1)))
         self.rbf = torch.zeros(N, N, dtype=torch.float64, device=dev)
         self.rbp = torch.zeros(N, N, dtype=torch.float64, device=dev)
@@ -163,7 +164,7 @@ class Plane2d3vPlasmaSolver:
         n_sorts = n_sorts or self.n_sorts
         bg = self.ro_initial if (with_background and self.ion_model == "background") else None
         _lib.check(L.lcb_plasma_deposit(
-            st.n_per_sort, n_sorts, self.N, self.h, st.Ns, self.precision,
+            st.n_per_sort, n_sorts, self.N, self.h, st.Ns, self.dep_precision,
             st.x_init.data_ptr(), st.y_init.data_ptr(), st.x_offt.data_ptr(),
             st.y_offt.data_ptr(), st.px.data_ptr(), st.py.data_ptr(), st.pz.data_ptr(),
             st.q.data_ptr(), st.m.data_ptr(), _lib.ptr(bg),
@@ -198,7 +199,7 @@ class Plane2d3vPlasmaSolver:
                       out: CurrentSet, first: bool):
         a = _lib.MoveDepositArgs()
         a.n_per_sort, a.n_sorts, a.particles_side = prev.n_per_sort, self.n_sorts, prev.Ns
-        a.grid_steps, a.precision, a.first = self.N, self.precision, int(first)
+        a.grid_steps, a.precision, a.first = self.N, self.dep_precision, int(first)
         a.lattice_fineness = self.fineness
         a.xi_step, a.boundary, a.h = self.dxi, self.boundary, self.h
         for i in range(6):

@@ -1,0 +1,93 @@
+"""Admission and retirement logic of the request server, with the GPU member
+replaced by a host fake (no device needed)."""
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from lcodepy_b200 import batch  # noqa: E402
+
+
+class FakeMember:
+    def __init__(self, cfg, drv, device=None, name=None):
+        self.name = name
+        self.n_steps = cfg["steps"]
+        self.cells = cfg["cells"]
+        self.done = 0
+        self.ez = torch.zeros(self.n_steps)
+
+    @property
+    def finished(self):
+        return self.done >= self.n_steps
+
+    def step(self):
+        self.ez[self.done] = self.done
+        self.done += 1
+
+    def complete(self):
+        return self.finished
+
+    def release(self):
+        pass
+
+
+@pytest.fixture
+def fake(monkeypatch):
+    monkeypatch.setattr(batch, "Member", FakeMember)
+    monkeypatch.setattr(batch, "footprint_bytes", lambda cfg: cfg["bytes"])
+
+
+def req(steps, nbytes, cells=1):
+    return {"steps": steps, "bytes": nbytes, "cells": cells}
+
+
+def test_budget_and_slots_bound_admission(fake):
+    srv = batch.Server(hbm_budget_bytes=10, max_slots=2, device="cpu")
+    srv.submit("a", req(3, 6), None, arrival=0.0)
+    srv.submit("b", req(2, 4), None, arrival=0.0)
+    srv.submit("c", req(2, 1), None, arrival=0.0)
+    srv.poll()
+    assert [m.name for m in srv.running] == ["a", "b"]      # slots full
+    srv.tick(); srv.tick(); srv.retire()
+    assert "b" in srv.done and srv.used == 6
+    srv.poll()
+    assert [m.name for m in srv.running] == ["a", "c"]      # admitted while a runs
+    srv.run()
+    assert set(srv.done) == {"a", "b", "c"} and srv.used == 0
+
+
+def test_first_come_first_served_under_memory_pressure(fake):
+    srv = batch.Server(hbm_budget_bytes=10, max_slots=8, device="cpu")
+    srv.submit("big0", req(5, 8), None, arrival=0.0)
+    srv.submit("big1", req(2, 8), None, arrival=0.0)
+    srv.submit("small", req(2, 1), None, arrival=0.0)
+    srv.poll()
+    # small fits next to big0 but must not overtake big1
+    assert [m.name for m in srv.running] == ["big0"]
+    srv.run()
+    d = srv.done
+    assert d["big1"]["admitted"] <= d["small"]["admitted"]
+
+
+def test_oversized_request_runs_alone(fake):
+    srv = batch.Server(hbm_budget_bytes=4, max_slots=8, device="cpu")
+    srv.submit("huge", req(2, 100), None, arrival=0.0)
+    srv.run()
+    assert list(srv.done) == ["huge"]
+
+
+def test_results_and_arrivals(fake):
+    srv = batch.Server(hbm_budget_bytes=100, max_slots=4, device="cpu")
+    srv.submit("late", req(3, 1), None, arrival=0.05)
+    srv.submit("now", req(4, 1), None, arrival=0.0)
+    srv.run()
+    assert srv.done["late"]["admitted"] >= 0.05
+    assert list(srv.done["now"]["ez"]) == [0, 1, 2, 3]
+
+
+def test_request_stream_is_seeded():
+    a = batch.request_stream(n=20)
+    b = batch.request_stream(n=20)
+    assert [(r[0], r[2]['window-length'], r[3]) for r in a] == \
+           [(r[0], r[2]['window-length'], r[3]) for r in b]
+    arr = [r[0] for r in a]
+    assert arr == sorted(arr) and arr[0] > 0
