@@ -38,10 +38,11 @@ extern "C" {
 #define LCB_DEVERR_PLASMA_STENCIL 1  /* plasma stencil left the grid (NaN or runaway) */
 #define LCB_DEVERR_BEAM_STENCIL 2    /* beam stencil left the N*N array */
 #define LCB_DEVERR_CAPACITY 4        /* a device-side buffer would overflow */
+#define LCB_DEVERR_FIXED_RANGE 8     /* a deposit contribution near the fixed-point range */
 
 /* Precision modes for the field solver and deposition. */
 #define LCB_PREC_FP64 0   /* FP64 everywhere: the reference's arithmetic */
-#define LCB_PREC_MIXED 1  /* FP32 deposition and FP32 transforms; FP64 particles */
+#define LCB_PREC_MIXED 1  /* fixed-point deposition, FP32 transforms; FP64 particles */
 
 const char *lcb_last_error(void);
 int lcb_version(void);
@@ -83,7 +84,8 @@ int lcb_plasma_move_smart(int64_t n, double xi_step, double boundary, double h,
 /* Charge and current deposition of all sorts.  Outputs ro, jx, jy, jz are
  * (2, N, N) planes (plane s = sort s), zeroed here first.  When ro_initial
  * is not NULL (background ions) plane 1 of ro is set to it afterwards.
- * precision LCB_PREC_MIXED accumulates in FP32 and converts to FP64.
+ * precision LCB_PREC_MIXED accumulates 64-bit fixed-point sums (resolution
+ * 2^-32, exact and order independent) and converts them to FP64.
  * Replaces compute_rhoj, lcode/plasma3d/rhoj.py:11-20, with deposit_plasma,
  * weights.py:249-285, and its kernel deposit_plasma_cupy, weights.py:151-190. */
 int lcb_plasma_deposit(int64_t n_per_sort, int n_sorts, int grid_steps,

@@ -18,6 +18,7 @@ LCB_PREC_MIXED = 1
 DEVERR_PLASMA_STENCIL = 1
 DEVERR_BEAM_STENCIL = 2
 DEVERR_CAPACITY = 4
+DEVERR_FIXED_RANGE = 8
 
 _vp = C.c_void_p
 _i64 = C.c_int64

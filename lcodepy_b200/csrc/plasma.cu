@@ -175,6 +175,39 @@ __device__ __forceinline__ void tile_slot(int q, bool two_per_cell, int &ti, int
 // Deposit one particle's 25-point stencil (weights.py:151-190 arithmetic)
 // into the block's shared window, or straight into HBM when the stencil
 // leaves the window.  dep = false: nothing to deposit.
+// Accumulator of the mixed-precision deposit: every contribution is rounded
+// to a multiple of 2^-32 and summed as a 64-bit integer, so the sums are
+// exact and do not depend on the order of the atomics (an FP32 sum of the
+// ~100 contributions a cell receives rounds at the magnitude of the running
+// total, which for the electron density is the background ~1, and leaves a
+// systematic ~1e-7 error that the background ions then expose).  The range
+// is +-2^31; particles whose contributions could approach it raise
+// LCB_DEVERR_FIXED_RANGE.
+constexpr double FIX_SCALE = 4294967296.0;            // 2^32
+constexpr double FIX_INV = 1.0 / 4294967296.0;
+constexpr double FIX_PARTICLE_LIMIT = 268435456.0;    // 2^28 per contribution
+typedef unsigned long long fix_t;
+
+template <typename Acc>
+__device__ __forceinline__ Acc to_acc(double v) { return Acc(v); }
+template <>
+__device__ __forceinline__ fix_t to_acc<fix_t>(double v)
+{
+    return (fix_t)__double2ll_rn(v * FIX_SCALE);
+}
+
+// Particles whose largest contribution could leave the fixed-point range
+// (|value| * max weight > 2^28) set the error word; nothing else changes.
+template <typename Acc>
+__device__ __forceinline__ void check_range(double, double, double, double, double, int *) {}
+template <>
+__device__ __forceinline__ void check_range<fix_t>(double dro, double djx, double djy, double djz,
+                                                   double ih, int *err)
+{
+    const double m = fmax(fmax(fabs(dro), fabs(djx)), fmax(fabs(djy), fabs(djz))) * ih * ih;
+    if (!(m < FIX_PARTICLE_LIMIT) && err) atomicOr(err, LCB_DEVERR_FIXED_RANGE);
+}
+
 template <typename Acc, int WX, int WY>
 __device__ __forceinline__ void deposit_one(Acc *sw, Acc *gro, Acc *gjx, Acc *gjy, Acc *gjz,
                                             int N, double h, int wx0, int wy0, bool dep,
@@ -200,16 +233,16 @@ __device__ __forceinline__ void deposit_one(Acc *sw, Acc *gro, Acc *gjx, Acc *gj
             const double w = wxa * wy[b];
             if (inwin) {
                 const int c = (lx + a) * WY + ly + b;
-                atomicAdd(sw + c, Acc(dro * w));
-                atomicAdd(sw + WSZ + c, Acc(djx * w));
-                atomicAdd(sw + 2 * WSZ + c, Acc(djy * w));
-                atomicAdd(sw + 3 * WSZ + c, Acc(djz * w));
+                atomicAdd(sw + c, to_acc<Acc>(dro * w));
+                atomicAdd(sw + WSZ + c, to_acc<Acc>(djx * w));
+                atomicAdd(sw + 2 * WSZ + c, to_acc<Acc>(djy * w));
+                atomicAdd(sw + 3 * WSZ + c, to_acc<Acc>(djz * w));
             } else {
                 const int64_t c = (int64_t)(ix + a - 2) * N + iy + b - 2;
-                atomicAdd(gro + c, Acc(dro * w));
-                atomicAdd(gjx + c, Acc(djx * w));
-                atomicAdd(gjy + c, Acc(djy * w));
-                atomicAdd(gjz + c, Acc(djz * w));
+                atomicAdd(gro + c, to_acc<Acc>(dro * w));
+                atomicAdd(gjx + c, to_acc<Acc>(djx * w));
+                atomicAdd(gjy + c, to_acc<Acc>(djy * w));
+                atomicAdd(gjz + c, to_acc<Acc>(djz * w));
             }
         }
     }
@@ -269,6 +302,7 @@ k_deposit_tiled(int64_t n_per_sort, int Ns, int N, double h,
                 dro = q / (1 - pz * ig);
                 const double rg = dro * ig;
                 djx = px * rg; djy = py * rg; djz = pz * rg;
+                check_range<Acc>(dro, djx, djy, djz, 1.0 / h, err);
                 ix = cell_of((x_init[k] + x_offt[k]) / h + 0.5, half_n, xl);
                 iy = cell_of((y_init[k] + y_offt[k]) / h + 0.5, half_n, yl);
                 if (!(ix >= 2 && ix < N - 2 && iy >= 2 && iy < N - 2)) {
@@ -484,6 +518,7 @@ k_move_deposit(int64_t n_per_sort, int Ns, int N, double h, double xi_step, doub
                     dro = qk / (1 - pz * igd);
                     const double rg = dro * igd;
                     djx = px * rg; djy = py * rg; djz = pz * rg;
+                    check_range<Acc>(dro, djx, djy, djz, 1.0 / h, err);
                     jx2 = cell_of((xi0 + xo) / h + 0.5, half_n, xl2);
                     jy2 = cell_of((yi0 + yo) / h + 0.5, half_n, yl2);
                     if (jx2 >= 2 && jx2 < N - 2 && jy2 >= 2 && jy2 < N - 2) dep = true;
@@ -545,11 +580,26 @@ static int dispatch_move_deposit(const lcb_move_deposit_args *a, dim3 grid, Acc 
                     : launch_move_deposit<Acc, DEP_WX, DEP_WY, false>(a, grid, ro, jx, jy, jz, st);
 }
 
-__global__ void k_f32_to_f64(int64_t n, const float *__restrict__ a, double *__restrict__ b)
+// Fixed-point sums (4 quantities x 2 columns x N*N) to the FP64 outputs;
+// columns past n_sorts get the background ions (ro) or zero.
+__global__ void k_fix_finish(int64_t plane, int n_sorts, const fix_t *__restrict__ w,
+                             const double *__restrict__ ro_initial, double *ro, double *jx,
+                             double *jy, double *jz)
 {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x)
-        b[i] = (double)a[i];
+    double *outs[4] = {ro, jx, jy, jz};
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 2 * plane;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int col = (int)(t / plane);
+#pragma unroll
+        for (int qd = 0; qd < 4; qd++) {
+            double v;
+            if (col < n_sorts)
+                v = (double)(long long)w[qd * 2 * plane + t] * FIX_INV;
+            else
+                v = (qd == 0 && ro_initial) ? ro_initial[t - plane] : 0.0;
+            outs[qd][t] = v;
+        }
+    }
 }
 
 static int grid_for(int64_t n, int threads)
@@ -558,6 +608,44 @@ static int grid_for(int64_t n, int threads)
     const int64_t cap = (int64_t)sm_count() * 16;
     if (blocks > cap) blocks = cap;
     return (int)(blocks < 1 ? 1 : blocks);
+}
+
+// Mixed-precision deposit: fixed-point sums in the workspace, then one pass
+// to the FP64 outputs (background column included).
+static int deposit_fixed(int64_t n_per_sort, int n_sorts, int N, double h, int particles_side,
+                         const double *x_init, const double *y_init, const double *x_offt,
+                         const double *y_offt, const double *px, const double *py,
+                         const double *pz, const double *q, const double *m,
+                         const double *ro_initial, double *ro, double *jx, double *jy,
+                         double *jz, void *workspace, size_t workspace_bytes, int *err,
+                         cudaStream_t st)
+{
+    const size_t plane = (size_t)N * N;
+    LCB_REQUIRE(workspace && workspace_bytes >= (size_t)8 * plane * sizeof(fix_t),
+                "deposit workspace too small");
+    fix_t *w = static_cast<fix_t *>(workspace);
+    cudaError_t e = cudaMemsetAsync(w, 0, 8 * plane * sizeof(fix_t), st);
+    if (e != cudaSuccess) return cuda_check(e, "memset fixed-point sums");
+    if (n_per_sort > 0) {
+        const dim3 grid((particles_side + DEP_TJ - 1) / DEP_TJ,
+                        (particles_side + DEP_TI - 1) / DEP_TI, n_sorts);
+        const size_t sm = deposit_smem_bytes<fix_t>();
+        static bool attr = false;
+        if (!attr) {
+            e = cudaFuncSetAttribute(k_deposit_tiled<fix_t>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            if (e != cudaSuccess) return cuda_check(e, "deposit smem attribute");
+            attr = true;
+        }
+        k_deposit_tiled<fix_t><<<grid, DEP_THREADS, sm, st>>>(
+            n_per_sort, particles_side, N, h, x_init, y_init, x_offt, y_offt, px, py, pz, q, m,
+            w, w + 2 * plane, w + 4 * plane, w + 6 * plane, err);
+        LCB_LAUNCH_CHECK("k_deposit_tiled<fixed>");
+    }
+    k_fix_finish<<<grid_for(2 * plane, 256), 256, 0, st>>>(plane, n_sorts, w, ro_initial, ro,
+                                                           jx, jy, jz);
+    LCB_LAUNCH_CHECK("k_fix_finish");
+    return LCB_OK;
 }
 
 }  // namespace lcb
@@ -602,7 +690,7 @@ extern "C" int lcb_plasma_move_smart(
 extern "C" size_t lcb_plasma_deposit_workspace_bytes(int grid_steps, int precision)
 {
     if (precision == LCB_PREC_MIXED)
-        return (size_t)8 * grid_steps * grid_steps * sizeof(float);
+        return (size_t)8 * grid_steps * grid_steps * sizeof(fix_t);
     return 0;
 }
 
@@ -624,6 +712,10 @@ extern "C" int lcb_plasma_deposit(
     cudaStream_t st = as_stream(stream);
     const size_t plane = (size_t)N * N;
     const size_t bytes = 2 * plane * sizeof(double);
+    if (precision == LCB_PREC_MIXED)
+        return deposit_fixed(n_per_sort, n_sorts, N, h, particles_side, x_init, y_init, x_offt,
+                             y_offt, px, py, pz, q, m, ro_initial, ro, jx, jy, jz, workspace,
+                             workspace_bytes, err, st);
     for (double *p : {ro, jx, jy, jz}) {
         cudaError_t e = cudaMemsetAsync(p, 0, bytes, st);
         if (e != cudaSuccess) return cuda_check(e, "memset currents");
@@ -631,7 +723,7 @@ extern "C" int lcb_plasma_deposit(
     if (n_per_sort > 0) {
         dim3 grid((particles_side + DEP_TJ - 1) / DEP_TJ,
                   (particles_side + DEP_TI - 1) / DEP_TI, n_sorts);
-        if (precision == LCB_PREC_FP64) {
+        {
             const size_t sm = deposit_smem_bytes<double>();
             static bool attr = false;
             if (!attr) {
@@ -644,30 +736,6 @@ extern "C" int lcb_plasma_deposit(
                 n_per_sort, particles_side, N, h, x_init, y_init, x_offt, y_offt,
                 px, py, pz, q, m, ro, jx, jy, jz, err);
             LCB_LAUNCH_CHECK("k_deposit_tiled<double>");
-        } else {
-            LCB_REQUIRE(workspace && workspace_bytes >= lcb_plasma_deposit_workspace_bytes(N, precision),
-                        "deposit workspace too small");
-            float *w = static_cast<float *>(workspace);
-            cudaError_t e = cudaMemsetAsync(w, 0, 8 * plane * sizeof(float), st);
-            if (e != cudaSuccess) return cuda_check(e, "memset f32 currents");
-            const size_t sm = deposit_smem_bytes<float>();
-            static bool attr_f = false;
-            if (!attr_f) {
-                e = cudaFuncSetAttribute(k_deposit_tiled<float>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-                if (e != cudaSuccess) return cuda_check(e, "deposit smem attribute");
-                attr_f = true;
-            }
-            k_deposit_tiled<float><<<grid, DEP_THREADS, sm, st>>>(
-                n_per_sort, particles_side, N, h, x_init, y_init, x_offt, y_offt,
-                px, py, pz, q, m, w, w + 2 * plane, w + 4 * plane, w + 6 * plane, err);
-            LCB_LAUNCH_CHECK("k_deposit_tiled<float>");
-            const int64_t cnt = (int64_t)2 * plane;
-            double *outs[4] = {ro, jx, jy, jz};
-            for (int qd = 0; qd < 4; qd++) {
-                k_f32_to_f64<<<grid_for(cnt, 256), 256, 0, st>>>(cnt, w + qd * 2 * plane, outs[qd]);
-                LCB_LAUNCH_CHECK("k_f32_to_f64");
-            }
         }
     }
     if (ro_initial) {
@@ -691,34 +759,33 @@ extern "C" int lcb_plasma_move_deposit(const lcb_move_deposit_args *a, void *str
     for (int f = 0; f < 6; f++) LCB_REQUIRE(a->fields[f], "field plane %d is NULL", f);
     cudaStream_t st = as_stream(stream);
     const size_t plane = (size_t)N * N;
+    const dim3 grid((a->particles_side + DEP_TJ - 1) / DEP_TJ,
+                    (a->particles_side + DEP_TI - 1) / DEP_TI, a->n_sorts);
+    if (a->precision == LCB_PREC_MIXED) {
+        LCB_REQUIRE(a->workspace && a->workspace_bytes >= lcb_plasma_deposit_workspace_bytes(N, a->precision),
+                    "deposit workspace too small");
+        fix_t *w = static_cast<fix_t *>(a->workspace);
+        cudaError_t e = cudaMemsetAsync(w, 0, 8 * plane * sizeof(fix_t), st);
+        if (e != cudaSuccess) return cuda_check(e, "memset fixed-point sums");
+        if (a->n_per_sort > 0) {
+            const int rc = dispatch_move_deposit<fix_t>(a, grid, w, w + 2 * plane, w + 4 * plane,
+                                                        w + 6 * plane, st);
+            if (rc) return rc;
+            LCB_LAUNCH_CHECK("k_move_deposit<fixed>");
+        }
+        k_fix_finish<<<grid_for(2 * plane, 256), 256, 0, st>>>(
+            plane, a->n_sorts, w, a->ro_initial, a->ro, a->jx, a->jy, a->jz);
+        LCB_LAUNCH_CHECK("k_fix_finish");
+        return LCB_OK;
+    }
     for (double *p : {a->ro, a->jx, a->jy, a->jz}) {
         cudaError_t e = cudaMemsetAsync(p, 0, 2 * plane * sizeof(double), st);
         if (e != cudaSuccess) return cuda_check(e, "memset currents");
     }
     if (a->n_per_sort > 0) {
-        dim3 grid((a->particles_side + DEP_TJ - 1) / DEP_TJ,
-                  (a->particles_side + DEP_TI - 1) / DEP_TI, a->n_sorts);
-        if (a->precision == LCB_PREC_FP64) {
-            const int rc = dispatch_move_deposit<double>(a, grid, a->ro, a->jx, a->jy, a->jz, st);
-            if (rc) return rc;
-            LCB_LAUNCH_CHECK("k_move_deposit<double>");
-        } else {
-            LCB_REQUIRE(a->workspace && a->workspace_bytes >= lcb_plasma_deposit_workspace_bytes(N, a->precision),
-                        "deposit workspace too small");
-            float *w = static_cast<float *>(a->workspace);
-            cudaError_t e = cudaMemsetAsync(w, 0, 8 * plane * sizeof(float), st);
-            if (e != cudaSuccess) return cuda_check(e, "memset f32 currents");
-            const int rc = dispatch_move_deposit<float>(a, grid, w, w + 2 * plane, w + 4 * plane,
-                                                        w + 6 * plane, st);
-            if (rc) return rc;
-            LCB_LAUNCH_CHECK("k_move_deposit<float>");
-            const int64_t cnt = (int64_t)2 * plane;
-            double *outs[4] = {a->ro, a->jx, a->jy, a->jz};
-            for (int qd = 0; qd < 4; qd++) {
-                k_f32_to_f64<<<grid_for(cnt, 256), 256, 0, st>>>(cnt, w + qd * 2 * plane, outs[qd]);
-                LCB_LAUNCH_CHECK("k_f32_to_f64");
-            }
-        }
+        const int rc = dispatch_move_deposit<double>(a, grid, a->ro, a->jx, a->jy, a->jz, st);
+        if (rc) return rc;
+        LCB_LAUNCH_CHECK("k_move_deposit<double>");
     }
     if (a->ro_initial) {
         cudaError_t e = cudaMemcpyAsync(a->ro + plane, a->ro_initial, plane * sizeof(double),

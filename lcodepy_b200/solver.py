@@ -317,7 +317,10 @@ class Plane2d3vPlasmaSolver:
         e = int(self.err.item())
         if e:
             self.err.zero_()
-            raise RuntimeError(
-                f"device error word 0x{e:x}: a plasma particle stencil left the grid "
-                "(NaN or runaway particle)" if e & _lib.DEVERR_PLASMA_STENCIL else
-                f"device error word 0x{e:x}")
+            why = []
+            if e & _lib.DEVERR_PLASMA_STENCIL:
+                why.append("a plasma particle stencil left the grid (NaN or runaway particle)")
+            if e & _lib.DEVERR_FIXED_RANGE:
+                why.append("a deposit contribution approached the fixed-point range of the "
+                           "mixed-precision deposit (use 'deposit-precision': 'fp64')")
+            raise RuntimeError(f"device error word 0x{e:x}: " + "; ".join(why or ["unknown"]))

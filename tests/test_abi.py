@@ -35,4 +35,4 @@ def test_library_loads_without_gpu():
     L = _lib.load()
     assert L.lcb_version() >= 100
     assert L.lcb_compute_fields_workspace_bytes(129, 0) > 0
-    assert L.lcb_plasma_deposit_workspace_bytes(129, 1) == 8 * 129 * 129 * 4
+    assert L.lcb_plasma_deposit_workspace_bytes(129, 1) == 8 * 129 * 129 * 8  # int64 sums
