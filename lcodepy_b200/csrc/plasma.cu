@@ -180,24 +180,37 @@ __device__ __forceinline__ void tile_slot(int q, bool two_per_cell, int &ti, int
 // exact and do not depend on the order of the atomics (an FP32 sum of the
 // ~100 contributions a cell receives rounds at the magnitude of the running
 // total, which for the electron density is the background ~1, and leaves a
-// systematic ~1e-7 error that the background ions then expose).  The range
-// is +-2^31; particles whose contributions could approach it raise
-// LCB_DEVERR_FIXED_RANGE.
+// systematic ~1e-7 error that the background ions then expose).
+//
+// The rounding is one FMA: v * 2^32 + 1.5 * 2^52 has a unit in the last
+// place of exactly 1, so the sum's low mantissa bits are round(v * 2^32) in
+// two's complement, read off by subtracting the constant's bit pattern (no
+// float-to-integer conversion instruction).  That needs |v| < 2^19 per
+// contribution; particles whose values could approach it (|value| / h^2 >=
+// 2^20, weights are below 0.36) raise LCB_DEVERR_FIXED_RANGE.  Sums have the
+// range +-2^31.
 constexpr double FIX_SCALE = 4294967296.0;            // 2^32
 constexpr double FIX_INV = 1.0 / 4294967296.0;
-constexpr double FIX_PARTICLE_LIMIT = 268435456.0;    // 2^28 per contribution
+constexpr double FIX_MAGIC = 6755399441055744.0;      // 1.5 * 2^52
+constexpr double FIX_PARTICLE_LIMIT = 1048576.0;      // 2^20
 typedef unsigned long long fix_t;
+
+// round(v * 2^32) from fma(v, 2^32, FIX_MAGIC) (or any x = w * 2^32 * v + FIX_MAGIC)
+__device__ __forceinline__ fix_t fix_bits(double x)
+{
+    return (fix_t)__double_as_longlong(x) - (fix_t)0x4338000000000000ull;
+}
 
 template <typename Acc>
 __device__ __forceinline__ Acc to_acc(double v) { return Acc(v); }
 template <>
 __device__ __forceinline__ fix_t to_acc<fix_t>(double v)
 {
-    return (fix_t)__double2ll_rn(v * FIX_SCALE);
+    return fix_bits(fma(v, FIX_SCALE, FIX_MAGIC));
 }
 
-// Particles whose largest contribution could leave the fixed-point range
-// (|value| * max weight > 2^28) set the error word; nothing else changes.
+// Particles whose largest contribution could leave the fixed-point rounding
+// range set the error word; nothing else changes.
 template <typename Acc>
 __device__ __forceinline__ void check_range(double, double, double, double, double, int *) {}
 template <>
@@ -580,6 +593,290 @@ static int dispatch_move_deposit(const lcb_move_deposit_args *a, dim3 grid, Acc 
                     : launch_move_deposit<Acc, DEP_WX, DEP_WY, false>(a, grid, ro, jx, jy, jz, st);
 }
 
+// ---------------------------------------------------------------------------
+// Mixed-precision fused stage: the per-particle algorithm of k_move_deposit
+// with the arithmetic chosen by what each part feeds.  Coordinates and
+// momenta (the push, reflection and absorption) stay FP64.  The midpoint
+// gather reads an FP32 copy of the six field planes' window with FP32
+// weights: the planes themselves come from the FP32 field solve.  The
+// deposit keeps FP64 weights, scales each particle's four values by
+// 2^32 / h^2 once, and rounds every contribution to a 64-bit integer with
+// one FMA against FIX_MAGIC (no conversion instruction), summed with integer
+// atomics.  Sized for three blocks of 256 threads per SM.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void weights4f(float x, float w[5])
+{
+    const float x2 = x * x, x3 = x2 * x, x4 = x3 * x;
+    const float a = 0.5f - x, b = 0.5f + x;
+    const float r6 = 1.0f / 6.0f, r24 = 1.0f / 24.0f;
+    w[0] = a * a * a * a * r24;
+    w[1] = 19 / 96.f - 11 / 24.f * x + x2 * 0.25f + x3 * r6 - x4 * r6;
+    w[2] = 115 / 192.f - 5 / 8.f * x2 + x4 * 0.25f;
+    w[3] = 19 / 96.f + 11 / 24.f * x + x2 * 0.25f - x3 * r6 - x4 * r6;
+    w[4] = b * b * b * b * r24;
+}
+
+template <int WX, int WY, bool FIRST>
+__global__ void __launch_bounds__(DEP_THREADS, 3)
+k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, double boundary,
+                  const double *__restrict__ Exf, const double *__restrict__ Eyf,
+                  const double *__restrict__ Ezf, const double *__restrict__ Bxf,
+                  const double *__restrict__ Byf, const double *__restrict__ Bzf,
+                  const double *__restrict__ x_init, const double *__restrict__ y_init,
+                  const double *__restrict__ xo_p, const double *__restrict__ yo_p,
+                  const double *__restrict__ px_p, const double *__restrict__ py_p,
+                  const double *__restrict__ pz_p, const double *__restrict__ q_p,
+                  const double *__restrict__ m_a,
+                  double *q_f, double *xo_f, double *yo_f, double *px_f, double *py_f,
+                  double *pz_f, fix_t *ro, fix_t *jx, fix_t *jy, fix_t *jz, int *err)
+{
+    constexpr int WSZ = WX * WY;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    fix_t *sw = reinterpret_cast<fix_t *>(smem_raw);           // [4][WX][WY] deposit
+    float *sf = reinterpret_cast<float *>(sw + 4 * WSZ);       // [6][WX][WY] fields
+    const int s = blockIdx.z;
+    const int i0 = blockIdx.y * DEP_TI, j0 = blockIdx.x * DEP_TJ;
+    const int64_t base = (int64_t)s * n_per_sort;
+    const int half_n = N / 2;
+    const int64_t NN = (int64_t)N * N;
+    fix_t *gro = ro + s * NN, *gjx = jx + s * NN, *gjy = jy + s * NN, *gjz = jz + s * NN;
+    const double *fld[6] = {Exf, Eyf, Ezf, Bxf, Byf, Bzf};
+    const double ih = 1.0 / h;
+
+    double dummy;
+    const int64_t k0 = base + (int64_t)i0 * Ns + j0;
+    const int wx0 = cell_of(x_init[k0] / h + 0.5, half_n, dummy) - 2 - DEP_SLACK;
+    const int wy0 = cell_of(y_init[k0] / h + 0.5, half_n, dummy) - 2 - DEP_SLACK;
+    bool two = false;
+    if (i0 + 1 < Ns) {
+        const double d = x_init[k0 + Ns] - x_init[k0];
+        two = fabs(2 * d - h) < 0.25 * h;
+    }
+    for (int t = threadIdx.x; t < 4 * WSZ; t += blockDim.x) sw[t] = 0;
+    for (int t = threadIdx.x; t < WSZ; t += blockDim.x) {
+        const int gx = wx0 + t / WY, gy = wy0 + t % WY;
+        const bool in = gx >= 0 && gx < N && gy >= 0 && gy < N;
+        const int64_t g = (int64_t)gx * N + gy;
+#pragma unroll
+        for (int f = 0; f < 6; f++) sf[f * WSZ + t] = in ? (float)__ldg(fld[f] + g) : 0.f;
+    }
+    __syncthreads();
+
+#pragma unroll 1
+    for (int r = 0; r < DEP_PPT; r++) {
+        int ti, tj;
+        tile_slot(threadIdx.x + r * DEP_THREADS, two, ti, tj);
+        const int i = i0 + ti, j = j0 + tj;
+        if (!(i < Ns && j < Ns)) continue;
+        const int64_t k = base + (int64_t)i * Ns + j;
+        const double mk = m_a[k];
+        const double opx = px_p[k], opy = py_p[k], opz = pz_p[k];
+        const double xo0 = xo_p[k], yo0 = yo_p[k];
+        double qk, xof, yof;
+        if (FIRST) {
+            qk = q_p[k];
+            xof = xo0; yof = yo0;
+            if (mk != 0) {
+                const double gm = sqrt(mk * mk + opz * opz + opx * opx + opy * opy);
+                const double adv = xi_step / (gm - opz);
+                xof += opx * adv;
+                yof += opy * adv;
+            }
+        } else {
+            qk = q_f[k];
+            xof = xo_f[k]; yof = yo_f[k];
+        }
+        if (qk == 0) {
+            if (FIRST) {
+                xo_f[k] = xof; yo_f[k] = yof;
+                px_f[k] = opx; py_f[k] = opy; pz_f[k] = opz;
+                q_f[k] = qk;
+            }
+            continue;
+        }
+        const double xi0 = x_init[k], yi0 = y_init[k];
+        double px = opx, py = opy, pz = opz;
+        double xh = xi0 + (xo0 + xof) / 2;
+        double yh = yi0 + (yo0 + yof) / 2;
+        if (xh > boundary)  { xh =  2 * boundary - xh; px = py = pz = 0; }
+        if (xh < -boundary) { xh = -2 * boundary - xh; px = py = pz = 0; }
+        if (yh > boundary)  { yh =  2 * boundary - yh; px = py = pz = 0; }
+        if (yh < -boundary) { yh = -2 * boundary - yh; px = py = pz = 0; }
+        double Ex, Ey, Ez, Bx, By, Bz;
+        {
+            double xl, yl;
+            const int ix = cell_of(xh * ih + 0.5, half_n, xl);
+            const int iy = cell_of(yh * ih + 0.5, half_n, yl);
+            float fEx = 0, fEy = 0, fEz = 0, fBx = 0, fBy = 0, fBz = 0;
+            if (ix >= 2 && ix < N - 2 && iy >= 2 && iy < N - 2) {
+                float wx[5], wy[5];
+                weights4f((float)xl, wx);
+                weights4f((float)yl, wy);
+                const int lx = ix - 2 - wx0, ly = iy - 2 - wy0;
+                if (lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY) {
+#pragma unroll
+                    for (int a = 0; a < 5; a++) {
+                        const int row = (lx + a) * WY + ly;
+#pragma unroll
+                        for (int b = 0; b < 5; b++) {
+                            const float w = wx[a] * wy[b];
+                            const int c = row + b;
+                            fEx += sf[c] * w; fBx += sf[3 * WSZ + c] * w;
+                            fEy += sf[WSZ + c] * w; fBy += sf[4 * WSZ + c] * w;
+                            fEz += sf[2 * WSZ + c] * w; fBz += sf[5 * WSZ + c] * w;
+                        }
+                    }
+                } else {
+#pragma unroll 1
+                    for (int a = 0; a < 5; a++) {
+                        const int row = (ix + a - 2) * N + iy - 2;
+#pragma unroll
+                        for (int b = 0; b < 5; b++) {
+                            const float w = wx[a] * wy[b];
+                            const int idx = row + b;
+                            fEx += (float)__ldg(Exf + idx) * w; fBx += (float)__ldg(Bxf + idx) * w;
+                            fEy += (float)__ldg(Eyf + idx) * w; fBy += (float)__ldg(Byf + idx) * w;
+                            fEz += (float)__ldg(Ezf + idx) * w; fBz += (float)__ldg(Bzf + idx) * w;
+                        }
+                    }
+                }
+            } else if (err) {
+                atomicOr(err, LCB_DEVERR_PLASMA_STENCIL);
+            }
+            Ex = fEx; Ey = fEy; Ez = fEz; Bx = fBx; By = fBy; Bz = fBz;
+        }
+        double gm = sqrt(mk * mk + px * px + py * py + pz * pz);
+        double ig = 1.0 / gm;
+        double vx = px * ig, vy = py * ig, vz = pz * ig;
+        double f = qk * xi_step / (1 - vz);
+        double dpx = f * (Ex + vy * Bz - vz * By);
+        double dpy = f * (Ey - vx * Bz + vz * Bx);
+        double dpz = f * (Ez + vx * By - vy * Bx);
+        px = opx + dpx * 0.5; py = opy + dpy * 0.5; pz = opz + dpz * 0.5;
+        gm = sqrt(mk * mk + px * px + py * py + pz * pz);
+        ig = 1.0 / gm;
+        vx = px * ig; vy = py * ig; vz = pz * ig;
+        f = qk * xi_step / (1 - vz);
+        dpx = f * (Ex + vy * Bz - vz * By);
+        dpy = f * (Ey - vx * Bz + vz * Bx);
+        dpz = f * (Ez + vx * By - vy * Bx);
+        px = opx + dpx * 0.5; py = opy + dpy * 0.5; pz = opz + dpz * 0.5;
+        gm = sqrt(mk * mk + px * px + py * py + pz * pz);
+        const double adv = xi_step / (gm - pz);
+        double xo = xo0 + px * adv;
+        double yo = yo0 + py * adv;
+        px = opx + dpx; py = opy + dpy; pz = opz + dpz;
+        double x = xi0 + xo, y = yi0 + yo;
+        if (x > boundary)  { x =  2 * boundary - x; xo = x - xi0; px = py = pz = 0; }
+        if (x < -boundary) { x = -2 * boundary - x; xo = x - xi0; px = py = pz = 0; }
+        if (y > boundary)  { y =  2 * boundary - y; yo = y - yi0; px = py = pz = 0; }
+        if (y < -boundary) { y = -2 * boundary - y; yo = y - yi0; px = py = pz = 0; }
+        bool absorbed = false;
+        if (x >= boundary || x <= -boundary || y >= boundary || y <= -boundary) {
+            xo = yo = 0; px = py = pz = 0;
+            absorbed = true;
+        }
+        xo_f[k] = xo; yo_f[k] = yo;
+        px_f[k] = px; py_f[k] = py; pz_f[k] = pz;
+        if (FIRST || absorbed) q_f[k] = absorbed ? 0.0 : qk;
+        if (absorbed) continue;
+
+        // ---- deposit of the new state ----
+        const double gd = sqrt(mk * mk + px * px + py * py + pz * pz);
+        const double igd = 1.0 / gd;
+        const double dro = qk / (1 - pz * igd);
+        const double rg = dro * igd;
+        const double djx = px * rg, djy = py * rg, djz = pz * rg;
+        check_range<fix_t>(dro, djx, djy, djz, ih, err);
+        double xl, yl;
+        const int cx = cell_of((xi0 + xo) * ih + 0.5, half_n, xl);
+        const int cy = cell_of((yi0 + yo) * ih + 0.5, half_n, yl);
+        if (!(cx >= 2 && cx < N - 2 && cy >= 2 && cy < N - 2)) {
+            if (err) atomicOr(err, LCB_DEVERR_PLASMA_STENCIL);
+            continue;
+        }
+        const double sc = FIX_SCALE * ih * ih;
+        const double s_ro = dro * sc, s_jx = djx * sc, s_jy = djy * sc, s_jz = djz * sc;
+        double wx[5], wy[5];
+        weights4(xl, wx);
+        weights4(yl, wy);
+        const int lx = cx - 2 - wx0, ly = cy - 2 - wy0;
+        if (lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY) {
+#pragma unroll
+            for (int a = 0; a < 5; a++) {
+#pragma unroll
+                for (int b = 0; b < 5; b++) {
+                    const double w = wx[a] * wy[b];
+                    const int c = (lx + a) * WY + ly + b;
+                    atomicAdd(sw + c, fix_bits(fma(s_ro, w, FIX_MAGIC)));
+                    atomicAdd(sw + WSZ + c, fix_bits(fma(s_jx, w, FIX_MAGIC)));
+                    atomicAdd(sw + 2 * WSZ + c, fix_bits(fma(s_jy, w, FIX_MAGIC)));
+                    atomicAdd(sw + 3 * WSZ + c, fix_bits(fma(s_jz, w, FIX_MAGIC)));
+                }
+            }
+        } else {
+#pragma unroll 1
+            for (int a = 0; a < 5; a++) {
+#pragma unroll
+                for (int b = 0; b < 5; b++) {
+                    const double w = wx[a] * wy[b];
+                    const int64_t c = (int64_t)(cx + a - 2) * N + cy + b - 2;
+                    atomicAdd(gro + c, fix_bits(fma(s_ro, w, FIX_MAGIC)));
+                    atomicAdd(gjx + c, fix_bits(fma(s_jx, w, FIX_MAGIC)));
+                    atomicAdd(gjy + c, fix_bits(fma(s_jy, w, FIX_MAGIC)));
+                    atomicAdd(gjz + c, fix_bits(fma(s_jz, w, FIX_MAGIC)));
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < WSZ; t += blockDim.x) {
+        const int gx = wx0 + t / WY, gy = wy0 + t % WY;
+        if (gx < 0 || gx >= N || gy < 0 || gy >= N) continue;
+        const int64_t c = (int64_t)gx * N + gy;
+        const fix_t v0 = sw[t], v1 = sw[WSZ + t], v2 = sw[2 * WSZ + t], v3 = sw[3 * WSZ + t];
+        if (v0) atomicAdd(gro + c, v0);
+        if (v1) atomicAdd(gjx + c, v1);
+        if (v2) atomicAdd(gjy + c, v2);
+        if (v3) atomicAdd(gjz + c, v3);
+    }
+}
+
+template <int WX, int WY>
+static size_t move_deposit_mx_smem() { return (size_t)WX * WY * (6 * sizeof(float) + 4 * sizeof(fix_t)); }
+
+template <int WX, int WY, bool FIRST>
+static int launch_move_deposit_mx(const lcb_move_deposit_args *a, dim3 grid, fix_t *w,
+                                  size_t plane, cudaStream_t st)
+{
+    const size_t sm = move_deposit_mx_smem<WX, WY>();
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k_move_deposit_mx<WX, WY, FIRST>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return cuda_check(e, "move_deposit smem attribute");
+        attr = true;
+    }
+    const lcb_plasma_particles &p = a->prev, &f = a->full;
+    k_move_deposit_mx<WX, WY, FIRST><<<grid, DEP_THREADS, sm, st>>>(
+        a->n_per_sort, a->particles_side, a->grid_steps, a->h, a->xi_step, a->boundary,
+        a->fields[0], a->fields[1], a->fields[2], a->fields[3], a->fields[4], a->fields[5],
+        p.x_init, p.y_init, p.x_offt, p.y_offt, p.px, p.py, p.pz, p.q, p.m,
+        f.q, f.x_offt, f.y_offt, f.px, f.py, f.pz, w, w + 2 * plane, w + 4 * plane,
+        w + 6 * plane, a->err);
+    return LCB_OK;
+}
+
+static int dispatch_move_deposit_mx(const lcb_move_deposit_args *a, dim3 grid, fix_t *w,
+                                    size_t plane, cudaStream_t st)
+{
+    if (a->lattice_fineness >= 2)
+        return a->first ? launch_move_deposit_mx<20, 28, true>(a, grid, w, plane, st)
+                        : launch_move_deposit_mx<20, 28, false>(a, grid, w, plane, st);
+    return a->first ? launch_move_deposit_mx<DEP_WX, DEP_WY, true>(a, grid, w, plane, st)
+                    : launch_move_deposit_mx<DEP_WX, DEP_WY, false>(a, grid, w, plane, st);
+}
+
 // Fixed-point sums (4 quantities x 2 columns x N*N) to the FP64 outputs;
 // columns past n_sorts get the background ions (ro) or zero.
 __global__ void k_fix_finish(int64_t plane, int n_sorts, const fix_t *__restrict__ w,
@@ -768,10 +1065,9 @@ extern "C" int lcb_plasma_move_deposit(const lcb_move_deposit_args *a, void *str
         cudaError_t e = cudaMemsetAsync(w, 0, 8 * plane * sizeof(fix_t), st);
         if (e != cudaSuccess) return cuda_check(e, "memset fixed-point sums");
         if (a->n_per_sort > 0) {
-            const int rc = dispatch_move_deposit<fix_t>(a, grid, w, w + 2 * plane, w + 4 * plane,
-                                                        w + 6 * plane, st);
+            const int rc = dispatch_move_deposit_mx(a, grid, w, plane, st);
             if (rc) return rc;
-            LCB_LAUNCH_CHECK("k_move_deposit<fixed>");
+            LCB_LAUNCH_CHECK("k_move_deposit_mx");
         }
         k_fix_finish<<<grid_for(2 * plane, 256), 256, 0, st>>>(
             plane, a->n_sorts, w, a->ro_initial, a->ro, a->jx, a->jy, a->jz);
