@@ -616,6 +616,93 @@ __device__ __forceinline__ void weights4f(float x, float w[5])
     w[4] = b * b * b * b * r24;
 }
 
+// Row stride (in floats) of the FP32 field window: the two half-warps of a
+// warp work one cell apart along x, and a stride of 16 (mod 32) words puts
+// their loads on disjoint banks.
+template <int WY>
+struct FieldStride { static constexpr int v = ((WY + 15) / 32) * 32 + 16; };
+
+// Midpoint gather of one particle: FP32 weights, FP32 sums, from the window
+// when the stencil fits in it, else from the FP64 planes in HBM.
+template <int WX, int WY>
+__device__ __forceinline__ void gather_one(const float *sf, const double *const *fld, int N,
+                                           int wx0, int wy0, int ix, int iy, float xl, float yl,
+                                           float F[6])
+{
+    constexpr int FS = FieldStride<WY>::v, FSZ = WX * FS;
+    float wx[5], wy[5];
+    weights4f(xl, wx);
+    weights4f(yl, wy);
+    const int lx = ix - 2 - wx0, ly = iy - 2 - wy0;
+    if (lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY) {
+#pragma unroll
+        for (int a = 0; a < 5; a++) {
+#pragma unroll
+            for (int b = 0; b < 5; b++) {
+                const float w = wx[a] * wy[b];
+                const int c = (lx + a) * FS + ly + b;
+#pragma unroll
+                for (int f = 0; f < 6; f++) F[f] += sf[f * FSZ + c] * w;
+            }
+        }
+    } else {
+#pragma unroll 1
+        for (int a = 0; a < 5; a++) {
+            const int row = (ix + a - 2) * N + iy - 2;
+#pragma unroll
+            for (int b = 0; b < 5; b++) {
+                const float w = wx[a] * wy[b];
+#pragma unroll
+                for (int f = 0; f < 6; f++) F[f] += (float)__ldg(fld[f] + row + b) * w;
+            }
+        }
+    }
+}
+
+// Deposit of one particle's scaled values (FP64 weights, fixed-point sums).
+template <int WX, int WY>
+__device__ __forceinline__ void deposit_fix_one(fix_t *sw, fix_t *const *g, int N, int wx0,
+                                                int wy0, int cx, int cy, double xl, double yl,
+                                                const double sv[4])
+{
+    constexpr int WSZ = WX * WY;
+    double wx[5], wy[5];
+    weights4(xl, wx);
+    weights4(yl, wy);
+    const int lx = cx - 2 - wx0, ly = cy - 2 - wy0;
+    if (lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY) {
+#pragma unroll
+        for (int a = 0; a < 5; a++) {
+#pragma unroll
+            for (int b = 0; b < 5; b++) {
+                const double w = wx[a] * wy[b];
+                const int c = (lx + a) * WY + ly + b;
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    atomicAdd(sw + q * WSZ + c, fix_bits(fma(sv[q], w, FIX_MAGIC)));
+            }
+        }
+    } else {
+#pragma unroll 1
+        for (int a = 0; a < 5; a++) {
+#pragma unroll
+            for (int b = 0; b < 5; b++) {
+                const double w = wx[a] * wy[b];
+                const int64_t c = (int64_t)(cx + a - 2) * N + cy + b - 2;
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    atomicAdd(g[q] + c, fix_bits(fma(sv[q], w, FIX_MAGIC)));
+            }
+        }
+    }
+}
+
+// A thread owns two particles, lattice slots t and t + DEP_THREADS, which on
+// the 2 x 2 per cell lattice are the two lattice rows of one cell.  While
+// both sit in the same cell the window values of the gather are loaded once
+// for the two, and their deposits are added before the shared atomics (each
+// contribution is still rounded on its own: fma(sA, wA, fma(sB, wB, M)) adds
+// two integers), which halves the shared-memory traffic of both phases.
 template <int WX, int WY, bool FIRST>
 __global__ void __launch_bounds__(DEP_THREADS, 3)
 k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, double boundary,
@@ -630,25 +717,37 @@ k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, d
                   double *q_f, double *xo_f, double *yo_f, double *px_f, double *py_f,
                   double *pz_f, fix_t *ro, fix_t *jx, fix_t *jy, fix_t *jz, int *err)
 {
+    static_assert(DEP_PPT == 2, "a thread owns two particles");
     constexpr int WSZ = WX * WY;
+    constexpr int FS = FieldStride<WY>::v, FSZ = WX * FS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     fix_t *sw = reinterpret_cast<fix_t *>(smem_raw);           // [4][WX][WY] deposit
-    float *sf = reinterpret_cast<float *>(sw + 4 * WSZ);       // [6][WX][WY] fields
+    float *sf = reinterpret_cast<float *>(sw + 4 * WSZ);       // [6][WX][FS] fields
     const int s = blockIdx.z;
-    const int i0 = blockIdx.y * DEP_TI, j0 = blockIdx.x * DEP_TJ;
     const int64_t base = (int64_t)s * n_per_sort;
     const int half_n = N / 2;
     const int64_t NN = (int64_t)N * N;
-    fix_t *gro = ro + s * NN, *gjx = jx + s * NN, *gjy = jy + s * NN, *gjz = jz + s * NN;
-    const double *fld[6] = {Exf, Eyf, Ezf, Bxf, Byf, Bzf};
+    fix_t *const g4[4] = {ro + s * NN, jx + s * NN, jy + s * NN, jz + s * NN};
+    const double *const fld[6] = {Exf, Eyf, Ezf, Bxf, Byf, Bzf};
     const double ih = 1.0 / h;
 
+    // Tiles start on a lattice row whose cell also holds the next row, so
+    // that a thread's two rows (ti, ti + 1 with ti even) share a cell: when
+    // rows 0 and 1 sit in different cells the tiles are shifted up by one
+    // row (the grid has one spare row of tiles for it).
     double dummy;
-    const int64_t k0 = base + (int64_t)i0 * Ns + j0;
+    int off = 0;
+    if (Ns > 1 && cell_of(x_init[base] / h + 0.5, half_n, dummy) !=
+                  cell_of(x_init[base + Ns] / h + 0.5, half_n, dummy))
+        off = 1;
+    const int i0 = blockIdx.y * DEP_TI - off, j0 = blockIdx.x * DEP_TJ;
+    const int ir = i0 < 0 ? 0 : i0;
+    if (ir >= Ns) return;
+    const int64_t k0 = base + (int64_t)ir * Ns + j0;
     const int wx0 = cell_of(x_init[k0] / h + 0.5, half_n, dummy) - 2 - DEP_SLACK;
     const int wy0 = cell_of(y_init[k0] / h + 0.5, half_n, dummy) - 2 - DEP_SLACK;
     bool two = false;
-    if (i0 + 1 < Ns) {
+    if (ir + 1 < Ns) {
         const double d = x_init[k0 + Ns] - x_init[k0];
         two = fabs(2 * d - h) < 0.25 * h;
     }
@@ -657,23 +756,33 @@ k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, d
         const int gx = wx0 + t / WY, gy = wy0 + t % WY;
         const bool in = gx >= 0 && gx < N && gy >= 0 && gy < N;
         const int64_t g = (int64_t)gx * N + gy;
+        const int c = (t / WY) * FS + t % WY;
 #pragma unroll
-        for (int f = 0; f < 6; f++) sf[f * WSZ + t] = in ? (float)__ldg(fld[f] + g) : 0.f;
+        for (int f = 0; f < 6; f++) sf[f * FSZ + c] = in ? (float)__ldg(fld[f] + g) : 0.f;
     }
     __syncthreads();
 
-#pragma unroll 1
-    for (int r = 0; r < DEP_PPT; r++) {
+    // ---- phase 1: K1 (first stage) and the midpoint of each particle ----
+    int64_t kk[2];
+    bool live[2], zero_p[2];
+    int ix[2], iy[2];
+    float xlf[2], ylf[2];
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
         int ti, tj;
-        tile_slot(threadIdx.x + r * DEP_THREADS, two, ti, tj);
+        tile_slot(threadIdx.x + p * DEP_THREADS, two, ti, tj);
         const int i = i0 + ti, j = j0 + tj;
-        if (!(i < Ns && j < Ns)) continue;
-        const int64_t k = base + (int64_t)i * Ns + j;
-        const double mk = m_a[k];
-        const double opx = px_p[k], opy = py_p[k], opz = pz_p[k];
+        live[p] = i >= 0 && i < Ns && j < Ns;
+        zero_p[p] = false;
+        ix[p] = iy[p] = -1000;
+        xlf[p] = ylf[p] = 0.f;
+        kk[p] = base + (int64_t)i * Ns + j;
+        if (!live[p]) continue;
+        const int64_t k = kk[p];
         const double xo0 = xo_p[k], yo0 = yo_p[k];
         double qk, xof, yof;
         if (FIRST) {
+            const double mk = m_a[k], opx = px_p[k], opy = py_p[k], opz = pz_p[k];
             qk = q_p[k];
             xof = xo0; yof = yo0;
             if (mk != 0) {
@@ -682,69 +791,83 @@ k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, d
                 xof += opx * adv;
                 yof += opy * adv;
             }
-        } else {
-            qk = q_f[k];
-            xof = xo_f[k]; yof = yo_f[k];
-        }
-        if (qk == 0) {
-            if (FIRST) {
+            if (qk == 0) {
                 xo_f[k] = xof; yo_f[k] = yof;
                 px_f[k] = opx; py_f[k] = opy; pz_f[k] = opz;
                 q_f[k] = qk;
             }
-            continue;
+        } else {
+            qk = q_f[k];
+            xof = xo_f[k]; yof = yo_f[k];
         }
-        const double xi0 = x_init[k], yi0 = y_init[k];
-        double px = opx, py = opy, pz = opz;
-        double xh = xi0 + (xo0 + xof) / 2;
-        double yh = yi0 + (yo0 + yof) / 2;
-        if (xh > boundary)  { xh =  2 * boundary - xh; px = py = pz = 0; }
-        if (xh < -boundary) { xh = -2 * boundary - xh; px = py = pz = 0; }
-        if (yh > boundary)  { yh =  2 * boundary - yh; px = py = pz = 0; }
-        if (yh < -boundary) { yh = -2 * boundary - yh; px = py = pz = 0; }
-        double Ex, Ey, Ez, Bx, By, Bz;
-        {
-            double xl, yl;
-            const int ix = cell_of(xh * ih + 0.5, half_n, xl);
-            const int iy = cell_of(yh * ih + 0.5, half_n, yl);
-            float fEx = 0, fEy = 0, fEz = 0, fBx = 0, fBy = 0, fBz = 0;
-            if (ix >= 2 && ix < N - 2 && iy >= 2 && iy < N - 2) {
-                float wx[5], wy[5];
-                weights4f((float)xl, wx);
-                weights4f((float)yl, wy);
-                const int lx = ix - 2 - wx0, ly = iy - 2 - wy0;
-                if (lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY) {
+        if (qk == 0) { live[p] = false; continue; }
+        double xh = x_init[k] + (xo0 + xof) / 2;
+        double yh = y_init[k] + (yo0 + yof) / 2;
+        bool z = false;
+        if (xh > boundary)  { xh =  2 * boundary - xh; z = true; }
+        if (xh < -boundary) { xh = -2 * boundary - xh; z = true; }
+        if (yh > boundary)  { yh =  2 * boundary - yh; z = true; }
+        if (yh < -boundary) { yh = -2 * boundary - yh; z = true; }
+        zero_p[p] = z;
+        double xl, yl;
+        ix[p] = cell_of(xh * ih + 0.5, half_n, xl);
+        iy[p] = cell_of(yh * ih + 0.5, half_n, yl);
+        xlf[p] = (float)xl; ylf[p] = (float)yl;
+        if (!(ix[p] >= 2 && ix[p] < N - 2 && iy[p] >= 2 && iy[p] < N - 2)) {
+            if (err) atomicOr(err, LCB_DEVERR_PLASMA_STENCIL);
+            ix[p] = -1000;  // no gather: zero fields, as in the reference's skip
+        }
+    }
+
+    // ---- phase 2: gather ----
+    float F0[6] = {0, 0, 0, 0, 0, 0}, F1[6] = {0, 0, 0, 0, 0, 0};
+    {
+        const int lx = ix[0] - 2 - wx0, ly = iy[0] - 2 - wy0;
+        const bool joint = ix[0] >= 0 && ix[0] == ix[1] && iy[0] == iy[1] &&
+                           lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY;
+        if (joint) {
+            float ax[5], ay[5], bx[5], by[5];
+            weights4f(xlf[0], ax); weights4f(ylf[0], ay);
+            weights4f(xlf[1], bx); weights4f(ylf[1], by);
 #pragma unroll
-                    for (int a = 0; a < 5; a++) {
-                        const int row = (lx + a) * WY + ly;
+            for (int a = 0; a < 5; a++) {
 #pragma unroll
-                        for (int b = 0; b < 5; b++) {
-                            const float w = wx[a] * wy[b];
-                            const int c = row + b;
-                            fEx += sf[c] * w; fBx += sf[3 * WSZ + c] * w;
-                            fEy += sf[WSZ + c] * w; fBy += sf[4 * WSZ + c] * w;
-                            fEz += sf[2 * WSZ + c] * w; fBz += sf[5 * WSZ + c] * w;
-                        }
-                    }
-                } else {
-#pragma unroll 1
-                    for (int a = 0; a < 5; a++) {
-                        const int row = (ix + a - 2) * N + iy - 2;
+                for (int b = 0; b < 5; b++) {
+                    const float wa = ax[a] * ay[b], wb = bx[a] * by[b];
+                    const int c = (lx + a) * FS + ly + b;
 #pragma unroll
-                        for (int b = 0; b < 5; b++) {
-                            const float w = wx[a] * wy[b];
-                            const int idx = row + b;
-                            fEx += (float)__ldg(Exf + idx) * w; fBx += (float)__ldg(Bxf + idx) * w;
-                            fEy += (float)__ldg(Eyf + idx) * w; fBy += (float)__ldg(Byf + idx) * w;
-                            fEz += (float)__ldg(Ezf + idx) * w; fBz += (float)__ldg(Bzf + idx) * w;
-                        }
+                    for (int f = 0; f < 6; f++) {
+                        const float v = sf[f * FSZ + c];
+                        F0[f] += v * wa;
+                        F1[f] += v * wb;
                     }
                 }
-            } else if (err) {
-                atomicOr(err, LCB_DEVERR_PLASMA_STENCIL);
             }
-            Ex = fEx; Ey = fEy; Ez = fEz; Bx = fBx; By = fBy; Bz = fBz;
+        } else {
+            if (ix[0] >= 0)
+                gather_one<WX, WY>(sf, fld, N, wx0, wy0, ix[0], iy[0], xlf[0], ylf[0], F0);
+            if (ix[1] >= 0)
+                gather_one<WX, WY>(sf, fld, N, wx0, wy0, ix[1], iy[1], xlf[1], ylf[1], F1);
         }
+    }
+
+    // ---- phase 3: push (FP64) and the deposit values ----
+    double sv[2][4];
+    int cx[2], cy[2];
+    double dxl[2], dyl[2];
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+        cx[p] = -1000; cy[p] = 0; dxl[p] = dyl[p] = 0;
+        sv[p][0] = sv[p][1] = sv[p][2] = sv[p][3] = 0;
+        if (!live[p]) continue;
+        const int64_t k = kk[p];
+        const float *Fp = p ? F1 : F0;
+        const double Ex = Fp[0], Ey = Fp[1], Ez = Fp[2], Bx = Fp[3], By = Fp[4], Bz = Fp[5];
+        const double mk = m_a[k], qk = FIRST ? q_p[k] : q_f[k];
+        const double opx = px_p[k], opy = py_p[k], opz = pz_p[k];
+        const double xi0 = x_init[k], yi0 = y_init[k];
+        double px = opx, py = opy, pz = opz;
+        if (zero_p[p]) px = py = pz = 0;
         double gm = sqrt(mk * mk + px * px + py * py + pz * pz);
         double ig = 1.0 / gm;
         double vx = px * ig, vy = py * ig, vz = pz * ig;
@@ -763,8 +886,8 @@ k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, d
         px = opx + dpx * 0.5; py = opy + dpy * 0.5; pz = opz + dpz * 0.5;
         gm = sqrt(mk * mk + px * px + py * py + pz * pz);
         const double adv = xi_step / (gm - pz);
-        double xo = xo0 + px * adv;
-        double yo = yo0 + py * adv;
+        double xo = xo_p[k] + px * adv;
+        double yo = yo_p[k] + py * adv;
         px = opx + dpx; py = opy + dpy; pz = opz + dpz;
         double x = xi0 + xo, y = yi0 + yo;
         if (x > boundary)  { x =  2 * boundary - x; xo = x - xi0; px = py = pz = 0; }
@@ -780,53 +903,49 @@ k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, d
         px_f[k] = px; py_f[k] = py; pz_f[k] = pz;
         if (FIRST || absorbed) q_f[k] = absorbed ? 0.0 : qk;
         if (absorbed) continue;
-
-        // ---- deposit of the new state ----
         const double gd = sqrt(mk * mk + px * px + py * py + pz * pz);
         const double igd = 1.0 / gd;
         const double dro = qk / (1 - pz * igd);
         const double rg = dro * igd;
         const double djx = px * rg, djy = py * rg, djz = pz * rg;
         check_range<fix_t>(dro, djx, djy, djz, ih, err);
-        double xl, yl;
-        const int cx = cell_of((xi0 + xo) * ih + 0.5, half_n, xl);
-        const int cy = cell_of((yi0 + yo) * ih + 0.5, half_n, yl);
-        if (!(cx >= 2 && cx < N - 2 && cy >= 2 && cy < N - 2)) {
+        const int c_x = cell_of((xi0 + xo) * ih + 0.5, half_n, dxl[p]);
+        const int c_y = cell_of((yi0 + yo) * ih + 0.5, half_n, dyl[p]);
+        if (!(c_x >= 2 && c_x < N - 2 && c_y >= 2 && c_y < N - 2)) {
             if (err) atomicOr(err, LCB_DEVERR_PLASMA_STENCIL);
             continue;
         }
+        cx[p] = c_x; cy[p] = c_y;
         const double sc = FIX_SCALE * ih * ih;
-        const double s_ro = dro * sc, s_jx = djx * sc, s_jy = djy * sc, s_jz = djz * sc;
-        double wx[5], wy[5];
-        weights4(xl, wx);
-        weights4(yl, wy);
-        const int lx = cx - 2 - wx0, ly = cy - 2 - wy0;
-        if (lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY) {
+        sv[p][0] = dro * sc; sv[p][1] = djx * sc; sv[p][2] = djy * sc; sv[p][3] = djz * sc;
+    }
+
+    // ---- phase 4: deposit ----
+    {
+        const int lx = cx[0] - 2 - wx0, ly = cy[0] - 2 - wy0;
+        const bool joint = cx[0] >= 0 && cx[0] == cx[1] && cy[0] == cy[1] &&
+                           lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY;
+        if (joint) {
+            double ax[5], ay[5], bx[5], by[5];
+            weights4(dxl[0], ax); weights4(dyl[0], ay);
+            weights4(dxl[1], bx); weights4(dyl[1], by);
 #pragma unroll
             for (int a = 0; a < 5; a++) {
 #pragma unroll
                 for (int b = 0; b < 5; b++) {
-                    const double w = wx[a] * wy[b];
+                    const double wa = ax[a] * ay[b], wb = bx[a] * by[b];
                     const int c = (lx + a) * WY + ly + b;
-                    atomicAdd(sw + c, fix_bits(fma(s_ro, w, FIX_MAGIC)));
-                    atomicAdd(sw + WSZ + c, fix_bits(fma(s_jx, w, FIX_MAGIC)));
-                    atomicAdd(sw + 2 * WSZ + c, fix_bits(fma(s_jy, w, FIX_MAGIC)));
-                    atomicAdd(sw + 3 * WSZ + c, fix_bits(fma(s_jz, w, FIX_MAGIC)));
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                        atomicAdd(sw + q * WSZ + c,
+                                  fix_bits(fma(sv[0][q], wa, fma(sv[1][q], wb, FIX_MAGIC))));
                 }
             }
         } else {
-#pragma unroll 1
-            for (int a = 0; a < 5; a++) {
-#pragma unroll
-                for (int b = 0; b < 5; b++) {
-                    const double w = wx[a] * wy[b];
-                    const int64_t c = (int64_t)(cx + a - 2) * N + cy + b - 2;
-                    atomicAdd(gro + c, fix_bits(fma(s_ro, w, FIX_MAGIC)));
-                    atomicAdd(gjx + c, fix_bits(fma(s_jx, w, FIX_MAGIC)));
-                    atomicAdd(gjy + c, fix_bits(fma(s_jy, w, FIX_MAGIC)));
-                    atomicAdd(gjz + c, fix_bits(fma(s_jz, w, FIX_MAGIC)));
-                }
-            }
+            if (cx[0] >= 0)
+                deposit_fix_one<WX, WY>(sw, g4, N, wx0, wy0, cx[0], cy[0], dxl[0], dyl[0], sv[0]);
+            if (cx[1] >= 0)
+                deposit_fix_one<WX, WY>(sw, g4, N, wx0, wy0, cx[1], cy[1], dxl[1], dyl[1], sv[1]);
         }
     }
     __syncthreads();
@@ -834,16 +953,19 @@ k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, d
         const int gx = wx0 + t / WY, gy = wy0 + t % WY;
         if (gx < 0 || gx >= N || gy < 0 || gy >= N) continue;
         const int64_t c = (int64_t)gx * N + gy;
-        const fix_t v0 = sw[t], v1 = sw[WSZ + t], v2 = sw[2 * WSZ + t], v3 = sw[3 * WSZ + t];
-        if (v0) atomicAdd(gro + c, v0);
-        if (v1) atomicAdd(gjx + c, v1);
-        if (v2) atomicAdd(gjy + c, v2);
-        if (v3) atomicAdd(gjz + c, v3);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const fix_t v = sw[q * WSZ + t];
+            if (v) atomicAdd(g4[q] + c, v);
+        }
     }
 }
 
 template <int WX, int WY>
-static size_t move_deposit_mx_smem() { return (size_t)WX * WY * (6 * sizeof(float) + 4 * sizeof(fix_t)); }
+static size_t move_deposit_mx_smem()
+{
+    return (size_t)WX * (FieldStride<WY>::v * 6 * sizeof(float) + WY * 4 * sizeof(fix_t));
+}
 
 template <int WX, int WY, bool FIRST>
 static int launch_move_deposit_mx(const lcb_move_deposit_args *a, dim3 grid, fix_t *w,
@@ -870,6 +992,7 @@ static int launch_move_deposit_mx(const lcb_move_deposit_args *a, dim3 grid, fix
 static int dispatch_move_deposit_mx(const lcb_move_deposit_args *a, dim3 grid, fix_t *w,
                                     size_t plane, cudaStream_t st)
 {
+    grid.y = (a->particles_side + 1 + DEP_TI - 1) / DEP_TI;  // spare row of tiles
     if (a->lattice_fineness >= 2)
         return a->first ? launch_move_deposit_mx<20, 28, true>(a, grid, w, plane, st)
                         : launch_move_deposit_mx<20, 28, false>(a, grid, w, plane, st);
