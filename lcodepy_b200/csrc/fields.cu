@@ -49,12 +49,52 @@ enum { OP_SE, OP_SO, OP_SET, OP_SOT, OP_CE, OP_CO, OP_CET, OP_COT,
 // elements so that every row starts on a 16-byte boundary (cp.async chunks).
 __host__ __device__ constexpr int ld2(int c) { return (c + 1) & ~1; }
 
+// The four int8 slices of x * scale (|x * scale| <= 1), each as a byte in the
+// low bits: the float sum with 1.5 * 2^23 rounds to an integer held in the
+// low mantissa bits.
+__device__ __forceinline__ void slice4(float x, float scale, unsigned sl[4])
+{
+    const float MG = 12582912.0f;
+    float u = x * scale * 64.f;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const float v = u + MG;
+        sl[i] = __float_as_uint(v) & 0xFFu;
+        u = (u - (v - MG)) * 128.f;
+    }
+}
+
+// The four slices packed in one 32-bit word, slice i in byte i: the form in
+// which the mixed-precision field solve stores transform blocks and folded
+// data (the same four bytes per element as FP32).
+__device__ __forceinline__ unsigned pack_slices(float x, float scale)
+{
+    unsigned sl[4];
+    slice4(x, scale, sl);
+    return sl[0] | (sl[1] << 8) | (sl[2] << 16) | (sl[3] << 24);
+}
+
+// Exponent E with m <= 2^E for m >= 0 (0 for m = 0).
+__device__ __forceinline__ int bound_exp(float m)
+{
+    if (!(m > 0.f)) return 0;
+    int e;
+    frexpf(m, &e);
+    return e;
+}
+
+
 struct OpLayout {
     int64_t off[OP_COUNT + 1];  // element offsets, 32-element aligned
     int64_t rows[OP_COUNT], cols[OP_COUNT], ld[OP_COUNT];
 };
 
-static OpLayout op_layout(int N)
+// Transform blocks: FP64 rows padded to an even length (16-byte cp.async
+// chunks); in mixed precision four int8 slice planes of rows x ld16(cols)
+// bytes each, i.e. rows x ld16(cols) FP32 words of storage.
+__host__ __device__ constexpr int ld16(int c) { return (c + 15) & ~15; }
+
+static OpLayout op_layout(int N, bool mixed = false)
 {
     const int n = N - 2;
     const int se = (n + 1) / 2, so = (n - 1) / 2, ce = (N + 1) / 2, co = (N - 1) / 2;
@@ -67,7 +107,7 @@ static OpLayout op_layout(int N)
         L.rows[i] = r[i];
         L.cols[i] = c[i];
         // transform blocks feed cp.async; solver matrices are read elementwise
-        L.ld[i] = i < OP_D ? ld2((int)c[i]) : c[i];
+        L.ld[i] = i < OP_D ? (mixed ? ld16((int)c[i]) : ld2((int)c[i])) : c[i];
         o += (r[i] * L.ld[i] + 31) / 32 * 32;
     }
     L.off[OP_COUNT] = o;
@@ -129,6 +169,39 @@ __global__ void k_build_ops(int N, double h, double c, OpLayout L, T *buf)
     }
 }
 
+// Mixed precision: the transform blocks as four int8 slice planes (bound 2).
+__global__ void k_build_slices(int N, OpLayout L, uint8_t *bytes)
+{
+    const int n = N - 2;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < L.off[OP_D];
+         e += (int64_t)gridDim.x * blockDim.x) {
+        int b = 0;
+        while (b < OP_D - 1 && e >= L.off[b + 1]) b++;
+        const int64_t loc = e - L.off[b];
+        const int64_t plane = L.rows[b] * L.ld[b];
+        if (loc >= plane) continue;          // alignment padding of the block
+        const int r = (int)(loc / L.ld[b]), q = (int)(loc % L.ld[b]);
+        double v = 0;
+        if (q < L.cols[b]) {
+            switch (b) {
+            case OP_SE: v = dst1(2 * r, q, n); break;
+            case OP_SO: v = dst1(2 * r + 1, q, n); break;
+            case OP_SET: v = dst1(2 * q, r, n); break;
+            case OP_SOT: v = dst1(2 * q + 1, r, n); break;
+            case OP_CE: v = dct1(2 * r, q, N); break;
+            case OP_CO: v = dct1(2 * r + 1, q, N); break;
+            case OP_CET: v = dct1(2 * q, r, N); break;
+            case OP_COT: v = dct1(2 * q + 1, r, N); break;
+            }
+        }
+        unsigned sl[4];
+        slice4((float)v, 0.5f, sl);
+        uint8_t *base = bytes + 4 * L.off[b];
+#pragma unroll
+        for (int i = 0; i < 4; i++) base[i * plane + loc] = (uint8_t)sl[i];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Batched GEMM descriptors.  Every product is a plain row-major
 // C (M x N) = A (M x K) * B (K x N); the even/odd folds are done by the
@@ -142,6 +215,13 @@ struct GemmDesc {
     int M, N, K;
     int rmul, radd, cmul, cadd;  // output element (m, n) -> (rmul m + radd, cmul n + cadd)
     int prob;             // problem id, for the field epilogue
+    // mixed precision: max |element| of a data operand (float bits, written
+    // by the fold pass that produced it); NULL for a transform block, whose
+    // elements are bounded by 2
+    const unsigned *amax_a, *amax_b;
+    // mixed precision: A and B are four int8 slice planes; lda / ldb are then
+    // row strides in bytes and a_plane / b_plane the plane strides in bytes
+    int a_plane, b_plane;
 };
 
 enum Epi { EPI_STORE = 0, EPI_SCALE = 1, EPI_FIELD = 2 };
@@ -161,6 +241,7 @@ struct GemmBatch {
     GemmDesc<T> d[MAXSUB];
     FieldOut out[NPROB];
     int grid_n;
+    unsigned *amax_out;   // mixed: per-problem max |stored value| (zeroed), or NULL
 };
 
 // Store one output element (m, n) of sub-product g; returns the value that
@@ -346,90 +427,309 @@ k_gemm_dmma(const __grid_constant__ GemmBatch<double> batch)
 }
 
 // ---------------------------------------------------------------------------
-// FP32 products (mixed precision) on the FP32 cores: BM x BN per CTA,
-// TM x TN outputs per thread, register-staged double buffering.
+// FP32 transforms on the 5th-generation tensor cores (mixed precision),
+// exact in integer arithmetic.  Every FP32 operand element is written as
+//     x = 2^E (s0 2^-6 + s1 2^-13 + s2 2^-20 + s3 2^-27),  |s_i| <= 64,
+// with E the exponent of its matrix's largest |element| (the fold pass that
+// produced the matrix records it; transform blocks are bounded by 2), so the
+// slices are int8 and the representation error is below 2^(E-28).  The
+// product of two such matrices is the sum over slice pairs (i, j) of int8
+// GEMMs scaled by 2^-(12 + 7(i+j)); the ten pairs with i + j <= 3 go to four
+// int32 accumulators in tensor memory (one per i + j), where tcgen05.mma
+// kind::i8 sums them exactly (|sum| < 4 * 64 * 64 * K < 2^31 for K < 2^17).
+// The epilogue combines the four in FP64: the result is as accurate as an
+// FP32 product and, unlike FP32 or TF32 tensor-core accumulation, free of
+// rounding bias and independent of summation order.
+//
+// CTA: 128 threads, a 128 x BN output tile in tensor memory (BN columns per
+// accumulator), K in stages of 32.  Every thread converts a share of the
+// stage's FP32 tiles into slices in shared memory (canonical no-swizzle
+// layouts: A K-major, core matrices of 8 rows x 16 bytes, 128 bytes apart
+// along K and 256 along M; B MN-major, core matrices of 8 K-rows x 16
+// bytes, 128 bytes apart along K and 512 along N); thread 0 issues the ten
+// MMAs and commits them to the stage's mbarrier, which the threads wait on
+// before refilling that stage's buffers two stages later.
 // ---------------------------------------------------------------------------
-template <int BM, int BN, int BK, int TM, int TN, int EPI>
-__global__ void __launch_bounds__((BM / TM) * (BN / TN))
-k_gemm_f32(const __grid_constant__ GemmBatch<float> batch)
+constexpr int I8_BM = 128, I8_BK = 32, I8_NS = 4;
+constexpr int I8_A_SLICE = I8_BM * I8_BK;            // bytes per slice of the A tile
+
+__device__ __forceinline__ unsigned smem_u32(const void *p)
 {
-    constexpr int NT = (BM / TM) * (BN / TN);
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+// 64-bit shared-memory matrix descriptor, no swizzle (start, LBO, SBO in bytes).
+__device__ __forceinline__ uint64_t umma_desc(unsigned addr, unsigned lbo, unsigned sbo)
+{
+    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor: kind::i8, s32 accumulator, signed int8 A (K-major)
+// and B (MN-major), M = 128, N = BN.
+template <int BN>
+__device__ __forceinline__ unsigned i8_idesc()
+{
+    return (2u << 4) | (1u << 7) | (1u << 10) | (1u << 16) | ((unsigned)(BN >> 3) << 17) |
+           ((unsigned)(I8_BM >> 4) << 24);
+}
+
+// Exponent of an operand's bound: a data operand's recorded maximum, or 2
+// for a transform block.
+__device__ __forceinline__ int operand_exp(const unsigned *amax)
+{
+    // a fold output is bounded by twice its source's largest element
+    return amax ? bound_exp(2.f * __uint_as_float(*amax)) : 1;
+}
+
+__device__ __forceinline__ bool mbar_wait(unsigned mbar, unsigned parity)
+{
+    // bounded: a phase that never completes ends the wait after ~2^22 polls
+    for (int it = 0; it < (1 << 22); it++) {
+        unsigned done;
+        asm volatile("{\n.reg .pred P1;\nmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n"
+                     "selp.b32 %0, 1, 0, P1;\n}\n"
+                     : "=r"(done) : "r"(mbar), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Epilogue of the integer products, split so that a group of outputs can
+// load what it needs (scale factor, previous field) before storing.
+template <int EPI>
+__device__ __forceinline__ double epi_pre(const GemmBatch<float> &b, const GemmDesc<float> &g,
+                                          int m, int n)
+{
+    const int om = g.rmul * m + g.radd, on = g.cmul * n + g.cadd;
+    if (EPI == EPI_SCALE) return (double)g.E[(int64_t)om * g.lde + on];
+    if (EPI == EPI_FIELD) {
+        const FieldOut &o = b.out[g.prob];
+        if ((o.kind == 0 && o.full) || (o.kind == 1 && o.half))
+            return o.prev[(int64_t)(om + o.row_off) * b.grid_n + on + o.col_off];
+    }
+    return 0.0;
+}
+
+template <int EPI>
+__device__ __forceinline__ double epi_apply(const GemmBatch<float> &b, const GemmDesc<float> &g,
+                                            int m, int n, float v, double pre, float &vmax)
+{
+    const int om = g.rmul * m + g.radd, on = g.cmul * n + g.cadd;
+    if (EPI == EPI_STORE) {
+        g.C[(int64_t)om * g.ldc + on] = v;
+        vmax = fmaxf(vmax, fabsf(v));
+    } else if (EPI == EPI_SCALE) {
+        const float st = v * (float)pre;
+        g.C[(int64_t)om * g.ldc + on] = st;
+        vmax = fmaxf(vmax, fabsf(st));
+    } else {
+        const FieldOut &o = b.out[g.prob];
+        const int64_t off = (int64_t)(om + o.row_off) * b.grid_n + on + o.col_off;
+        const double dv = (double)v;
+        if (o.kind == 0) {
+            if (o.half) o.half[off] = dv;
+            if (o.full) o.full[off] = 2 * dv - pre;
+        } else if (o.kind == 1) {
+            if (o.full) o.full[off] = dv;
+            if (o.half) o.half[off] = (dv + pre) / 2;
+        } else if (o.kind == 2) {
+            if (o.full) o.full[off] = dv;
+            if (o.half) o.half[off] = dv;
+        } else {
+            o.bz_raw[off] = dv;
+            return dv;
+        }
+    }
+    return 0.0;
+}
+
+template <int BN>
+struct I8Cfg {
+    static constexpr int ST = 4;                                       // pipeline stages
+    static constexpr int B_SLICE = I8_BK * BN;                         // bytes
+    static constexpr int STAGE = I8_NS * (I8_A_SLICE + B_SLICE);       // bytes
+    static constexpr int TMEM_COLS = 4 * BN;                           // power of two
+    static constexpr size_t smem = (size_t)ST * STAGE + 64;
+};
+
+template <int BN, int EPI>
+__global__ void __launch_bounds__(128)
+k_gemm_i8(const __grid_constant__ GemmBatch<float> batch)
+{
+    using Cfg = I8Cfg<BN>;
+    constexpr int ST = Cfg::ST;
+    static_assert(Cfg::TMEM_COLS == 256 || Cfg::TMEM_COLS == 512, "tensor memory columns");
+    static_assert(4 * 32 * (BN + 1) * sizeof(float) <= (size_t)ST * Cfg::STAGE, "epilogue staging");
+    extern __shared__ __align__(1024) uint8_t i8sm[];
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(i8sm + ST * Cfg::STAGE);   // [ST]
+    unsigned *tslot = reinterpret_cast<unsigned *>(mbar + ST);
+
     const GemmDesc<float> &g = batch.d[blockIdx.z];
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-    if (m0 >= g.M || n0 >= g.N) return;
-    __shared__ float As[2][BK][BM + 4];
-    __shared__ float Bs[2][BK][BN];
-    const int tid = threadIdx.x;
-    const int tn = tid % (BN / TN), tm = tid / (BN / TN);
-    float acc[TM][TN];
-#pragma unroll
-    for (int i = 0; i < TM; i++)
-#pragma unroll
-        for (int j = 0; j < TN; j++) acc[i][j] = 0.f;
-    constexpr int A_PER = (BM * BK + NT - 1) / NT, B_PER = (BK * BN + NT - 1) / NT;
-    float ra[A_PER], rb[B_PER];
-    auto load_regs = [&](int k0) {
-#pragma unroll
-        for (int r = 0; r < A_PER; r++) {
-            const int e = tid + r * NT;
-            const int mm = e / BK, kk = e % BK;
-            const int gm = m0 + mm, gk = k0 + kk;
-            ra[r] = (e < BM * BK && gm < g.M && gk < g.K) ? g.A[(int64_t)gm * g.lda + gk] : 0.f;
-        }
-#pragma unroll
-        for (int r = 0; r < B_PER; r++) {
-            const int e = tid + r * NT;
-            const int kk = e / BN, nn = e % BN;
-            const int gk = k0 + kk, gn = n0 + nn;
-            rb[r] = (e < BK * BN && gk < g.K && gn < g.N) ? g.B[(int64_t)gk * g.ldb + gn] : 0.f;
-        }
-    };
-    auto store_smem = [&](int buf) {
-#pragma unroll
-        for (int r = 0; r < A_PER; r++) {
-            const int e = tid + r * NT;
-            if (e < BM * BK) As[buf][e % BK][e / BK] = ra[r];
-        }
-#pragma unroll
-        for (int r = 0; r < B_PER; r++) {
-            const int e = tid + r * NT;
-            if (e < BK * BN) Bs[buf][e / BN][e % BN] = rb[r];
-        }
-    };
-    const int nk = (g.K + BK - 1) / BK;
-    load_regs(0);
-    store_smem(0);
+    const int M = g.M, N = g.N, K = g.K;
+    const int m0 = blockIdx.y * I8_BM, n0 = blockIdx.x * BN;
+    if (m0 >= M || n0 >= N) return;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int ea = operand_exp(g.amax_a), eb = operand_exp(g.amax_b);
+    const uint8_t *Ab = reinterpret_cast<const uint8_t *>(g.A);
+    const uint8_t *Bb = reinterpret_cast<const uint8_t *>(g.B);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(tslot)), "r"(Cfg::TMEM_COLS) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0)
+        for (int q = 0; q < ST; q++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(mbar + q)), "r"(1)
+                         : "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const unsigned tmem = *tslot;
+    const unsigned idesc = i8_idesc<BN>();
+
+    // one stage: A rows m0.. (K-major cores), B rows k0.. (MN-major cores),
+    // 16-byte chunks of the slice planes, zero past the matrix edges
+    auto issue = [&](int buf, int kt) {
+        uint8_t *sA = i8sm + buf * Cfg::STAGE;
+        uint8_t *sB = sA + I8_NS * I8_A_SLICE;
+        const int k0 = kt * I8_BK;
+#pragma unroll
+        for (int c = tid; c < I8_NS * I8_BM * 2; c += 128) {
+            const int sl = c / (2 * I8_BM), rem = c % (2 * I8_BM), r = rem >> 1, hk = rem & 1;
+            const int gm = m0 + r, gk = k0 + 16 * hk;
+            int bytes = gm < M ? K - gk : 0;
+            bytes = bytes < 0 ? 0 : (bytes > 16 ? 16 : bytes);
+            const uint8_t *src = bytes ? Ab + (int64_t)sl * g.a_plane + (int64_t)gm * g.lda + gk : Ab;
+            cp_async16(sA + sl * I8_A_SLICE + (r >> 3) * 256 + hk * 128 + (r & 7) * 16, src, bytes);
+        }
+#pragma unroll
+        for (int c = tid; c < I8_NS * I8_BK * (BN / 16); c += 128) {
+            const int sl = c / (I8_BK * (BN / 16)), rem = c % (I8_BK * (BN / 16));
+            const int kr = rem % I8_BK, nc = rem / I8_BK;
+            const int gk = k0 + kr, gn = n0 + 16 * nc;
+            int bytes = gk < K ? N - gn : 0;
+            bytes = bytes < 0 ? 0 : (bytes > 16 ? 16 : bytes);
+            const uint8_t *src = bytes ? Bb + (int64_t)sl * g.b_plane + (int64_t)gk * g.ldb + gn : Bb;
+            cp_async16(sB + sl * Cfg::B_SLICE + nc * 512 + (kr >> 3) * 128 + (kr & 7) * 16, src,
+                       bytes);
+        }
+    };
+
+    // loads run PF stages ahead; a buffer is refilled ST - PF stages after its
+    // MMAs were issued, so neither the copies nor the MMAs are waited on
+    // right after they start
+    constexpr int PF = 2;
+    static_assert(PF >= 1 && PF < ST, "pipeline depth");
+    const int nk = (K + I8_BK - 1) / I8_BK;
+#pragma unroll
+    for (int q = 0; q < PF; q++) {
+        if (q < nk) issue(q, q);
+        cp_async_commit();
+    }
+    bool ok = true;
     for (int kt = 0; kt < nk; kt++) {
-        const int buf = kt & 1;
-        if (kt + 1 < nk) load_regs((kt + 1) * BK);
-#pragma unroll
-        for (int kk = 0; kk < BK; kk++) {
-            float a[TM], b[TN];
-#pragma unroll
-            for (int i = 0; i < TM; i++) a[i] = As[buf][kk][tm * TM + i];
-#pragma unroll
-            for (int j = 0; j < TN; j++) b[j] = Bs[buf][kk][tn + j * (BN / TN)];
-#pragma unroll
-            for (int i = 0; i < TM; i++)
-#pragma unroll
-                for (int j = 0; j < TN; j++) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
-        }
-        if (kt + 1 < nk) store_smem(buf ^ 1);
+        const int buf = kt % ST;
+        cp_async_wait<PF - 1>();
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const unsigned a0 = smem_u32(i8sm + buf * Cfg::STAGE);
+            const unsigned b0 = a0 + I8_NS * I8_A_SLICE;
+#pragma unroll
+            for (int i = 0; i < I8_NS; i++) {
+#pragma unroll
+                for (int j = 0; j < I8_NS - i; j++) {
+                    const uint64_t da = umma_desc(a0 + i * I8_A_SLICE, 128, 256);
+                    const uint64_t db = umma_desc(b0 + j * Cfg::B_SLICE, 128, 512);
+                    const unsigned acc = tmem + (unsigned)((i + j) * BN);
+                    const unsigned en = (kt > 0 || i > 0) ? 1u : 0u;
+                    asm volatile("{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+                                 "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, "
+                                 "{%5, %5, %5, %5}, p;\n}\n"
+                                 :: "r"(acc), "l"(da), "l"(db), "r"(idesc), "r"(en), "r"(0u)
+                                 : "memory");
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         :: "r"(smem_u32(mbar + buf)) : "memory");
+        }
+        // refill the buffer of stage nxt - ST once its MMAs are done
+        const int nxt = kt + PF;
+        if (nxt < nk) {
+            if (nxt >= ST) ok &= mbar_wait(smem_u32(mbar + (nxt - ST) % ST), ((nxt - ST) / ST) & 1);
+            issue(nxt % ST, nxt);
+        }
+        cp_async_commit();
     }
-    double part = 0;
+    // the last commit covers every MMA issued before it
+    ok &= mbar_wait(smem_u32(mbar + (nk - 1) % ST), ((nk - 1) / ST) & 1);
+    cp_async_wait<0>();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+    // epilogue: warp w holds rows 32 w .. 32 w + 31 of the tile (its TMEM
+    // lanes); the combined values go through shared memory (the pipeline
+    // buffers are free now) so that the stores run along rows
+    float *stage = reinterpret_cast<float *>(i8sm) + warp * 32 * (BN + 1);
+    const double scale = ldexp(1.0, ea + eb - 12);
+#pragma unroll 1
+    for (int c8 = 0; c8 < BN / 8; c8++) {
+        unsigned r[4][8];
 #pragma unroll
-    for (int i = 0; i < TM; i++) {
-        const int gm = m0 + tm * TM + i;
-        if (gm >= g.M) continue;
+        for (int q = 0; q < 4; q++) {
+            const unsigned taddr = tmem + ((unsigned)(32 * warp) << 16) + (unsigned)(q * BN + 8 * c8);
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                         : "=r"(r[q][0]), "=r"(r[q][1]), "=r"(r[q][2]), "=r"(r[q][3]),
+                           "=r"(r[q][4]), "=r"(r[q][5]), "=r"(r[q][6]), "=r"(r[q][7])
+                         : "r"(taddr));
+        }
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int j = 0; j < TN; j++) {
-            const int gn = n0 + tn + j * (BN / TN);
-            if (gn < g.N) part += epilogue<float, EPI>(batch, g, gm, gn, acc[i][j]);
+        for (int e = 0; e < 8; e++) {
+            const double d = (double)(int)r[0][e] + ldexp((double)(int)r[1][e], -7) +
+                             ldexp((double)(int)r[2][e], -14) + ldexp((double)(int)r[3][e], -21);
+            stage[lane * (BN + 1) + 8 * c8 + e] = ok ? (float)(d * scale) : __int_as_float(0x7fc00000);
         }
     }
-    if (EPI == EPI_FIELD && batch.out[g.prob].kind == 3) bz_reduce<NT>(part, batch.out[g.prob].bz_sum);
+    __syncwarp();
+    double part = 0;
+    float vmax = 0.f;
+    // rows in groups of 8: the scale factors or previous fields they need
+    // are loaded for the whole group before any store
+    constexpr int CB = BN / 32;
+#pragma unroll 1
+    for (int r0 = 0; r0 < 32; r0 += 8) {
+        double pre[8][CB];
+#pragma unroll
+        for (int rr = 0; rr < 8; rr++)
+#pragma unroll
+            for (int cb = 0; cb < CB; cb++) {
+                const int gm = m0 + 32 * warp + r0 + rr, gn = n0 + 32 * cb + lane;
+                pre[rr][cb] = (gm < M && gn < N) ? epi_pre<EPI>(batch, g, gm, gn) : 0.0;
+            }
+#pragma unroll
+        for (int rr = 0; rr < 8; rr++)
+#pragma unroll
+            for (int cb = 0; cb < CB; cb++) {
+                const int gm = m0 + 32 * warp + r0 + rr, col = 32 * cb + lane, gn = n0 + col;
+                if (gm >= M || gn >= N) continue;
+                const float v = stage[(r0 + rr) * (BN + 1) + col];
+                part += epi_apply<EPI>(batch, g, gm, gn, v, pre[rr][cb], vmax);
+            }
+    }
+    if (EPI != EPI_FIELD && batch.amax_out) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+        if (lane == 0 && vmax > 0.f) atomicMax(batch.amax_out + g.prob, __float_as_uint(vmax));
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                     :: "r"(tmem), "r"(Cfg::TMEM_COLS) : "memory");
+    if (EPI == EPI_FIELD && batch.out[g.prob].kind == 3) bz_reduce<128>(part, batch.out[g.prob].bz_sum);
 }
 
 // ---------------------------------------------------------------------------
@@ -444,12 +744,91 @@ struct FoldDesc {
     const T *src;
     T *dst;
     int R, C, by_rows;
+    // mixed precision: the source's largest |element| (float bits); the
+    // output is then written as packed int8 slices scaled by the bound 2x that
+    const unsigned *src_max;
 };
 
 template <typename T>
 struct FoldBatch {
     FoldDesc<T> d[NPROB];
+    unsigned *clear;      // NPROB maxima zeroed here for the next producer, or NULL
 };
+
+// Mixed precision fold: FP32 source, int8 slice planes out.  A thread makes
+// four consecutive outputs of a row, one 32-bit store per plane.
+__device__ __forceinline__ void put_slices4(uint8_t *blk, int64_t plane, int64_t at,
+                                            const float v[4], float scale)
+{
+    unsigned w[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        unsigned sl[4];
+        slice4(v[e], scale, sl);
+#pragma unroll
+        for (int i = 0; i < 4; i++) w[i] |= sl[i] << (8 * e);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) *reinterpret_cast<unsigned *>(blk + i * plane + at) = w[i];
+}
+
+__global__ void __launch_bounds__(128) k_fold_slices(const __grid_constant__ FoldBatch<float> fb)
+{
+    const FoldDesc<float> &f = fb.d[blockIdx.z];
+    const int R = f.R, C = f.C, ldc = ld2(C);
+    if (fb.clear && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x < NPROB)
+        fb.clear[threadIdx.x] = 0u;
+    const float scale = ldexpf(1.f, -bound_exp(2.f * __uint_as_float(*f.src_max)));
+    uint8_t *blk = reinterpret_cast<uint8_t *>(f.dst);
+    for (int i = blockIdx.y; i < R; i += gridDim.y) {
+        if (!f.by_rows) {
+            const int he = (C + 1) / 2, ho = C - he, mid = (C - 1) / 2;
+            const int gu = (he + 3) / 4, gv = (ho + 3) / 4;
+            const float *row = f.src + (int64_t)i * ldc;
+            for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < gu + gv;
+                 t += gridDim.x * blockDim.x) {
+                float v[4];
+                if (t < gu) {
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        const int j = 4 * t + e;
+                        v[e] = j < mid ? row[j] + row[C - 1 - j] : (j == mid ? row[mid] : 0.f);
+                    }
+                    put_slices4(blk, (int64_t)R * ld16(he), (int64_t)i * ld16(he) + 4 * t, v, scale);
+                } else {
+                    const int tv = t - gu;
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        const int jj = 4 * tv + e;
+                        v[e] = jj < ho ? row[jj] - row[C - 1 - jj] : 0.f;
+                    }
+                    put_slices4(blk + 4 * (int64_t)R * ld16(he), (int64_t)R * ld16(ho),
+                                (int64_t)i * ld16(ho) + 4 * tv, v, scale);
+                }
+            }
+        } else {
+            const int he = (R + 1) / 2, ho = R - he, mid = (R - 1) / 2;
+            const int64_t ldb = ld16(C);
+            const float *ra = f.src + (int64_t)(i < he ? i : i - he) * ldc;
+            const float *rb = f.src + (int64_t)(i < he ? R - 1 - i : R - 1 - (i - he)) * ldc;
+            const bool single = i == mid && i < he;
+            for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < (C + 3) / 4;
+                 t += gridDim.x * blockDim.x) {
+                float v[4];
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const int j = 4 * t + e;
+                    v[e] = j >= C ? 0.f : (single ? ra[j] : (i < he ? ra[j] + rb[j] : ra[j] - rb[j]));
+                }
+                if (i < he)
+                    put_slices4(blk, (int64_t)he * ldb, (int64_t)i * ldb + 4 * t, v, scale);
+                else
+                    put_slices4(blk + 4 * (int64_t)he * ldb, (int64_t)ho * ldb,
+                                (int64_t)(i - he) * ldb + 4 * t, v, scale);
+            }
+        }
+    }
+}
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_fold(const __grid_constant__ FoldBatch<T> fb)
@@ -500,6 +879,7 @@ struct RhsArgs {
     const double *rb_full, *rb_prev;
     const double *Ex, *Ey, *Bx, *By;          // fields (Helmholtz term)
     double *bz_sum;
+    unsigned *amax_out;                       // mixed: per-output max |value| (zeroed), or NULL
     int with_phi;
 };
 
@@ -511,17 +891,77 @@ __device__ __forceinline__ double psum(const double *a, int np, int64_t plane, i
 constexpr int RHS_TY = 8, RHS_TX = 32;
 
 template <typename T>
+__device__ __forceinline__ void rhs_node(const RhsArgs &a, const double (*s_ro)[RHS_TX + 2],
+                                         const double (*s_jz)[RHS_TX + 2],
+                                         const double (*s_jx)[RHS_TX + 2],
+                                         const double (*s_jy)[RHS_TX + 2], int li, int lj, int i,
+                                         int j, T *X0, T *X1, T *X2, T *X3, T *X4, T *X5, T *X6,
+                                         float mx[NPROB])
+{
+    const int N = a.N, n = N - 2;
+    const int ldN = ld2(N), ldn = ld2(n);
+    const int64_t plane = (int64_t)N * N;
+    const int64_t t = (int64_t)i * N + j;
+    const bool inner = i >= 1 && i < N - 1 && j >= 1 && j < N - 1;
+    const double h2 = a.h * 2;
+    double dro_dx = 0, dro_dy = 0, djz_dx = 0, djz_dy = 0;
+    if (inner) {
+        dro_dx = (s_ro[li + 1][lj] - s_ro[li - 1][lj]) / h2;
+        dro_dy = (s_ro[li][lj + 1] - s_ro[li][lj - 1]) / h2;
+        djz_dx = (s_jz[li + 1][lj] - s_jz[li - 1][lj]) / h2;
+        djz_dy = (s_jz[li][lj + 1] - s_jz[li][lj - 1]) / h2;
+    }
+    const double djx_dxi = (psum(a.jx_p, a.n_p, plane, t) - s_jx[li][lj]) / a.dxi;
+    const double djy_dxi = (psum(a.jy_p, a.n_p, plane, t) - s_jy[li][lj]) / a.dxi;
+    const double Ex_rhs = -(dro_dx - djx_dxi - a.c * a.Ex[t]);
+    const double Ey_rhs = -(dro_dy - djy_dxi - a.c * a.Ey[t]);
+    const double Bx_rhs = +(djz_dy - djy_dxi + a.c * a.Bx[t]);
+    const double By_rhs = -(djz_dx - djx_dxi - a.c * a.By[t]);
+    if (i >= 1 && i < N - 1) {
+        const int64_t o = (int64_t)(i - 1) * ldN + j;
+        X0[o] = (T)Ey_rhs; mx[0] = fmaxf(mx[0], fabsf((float)Ey_rhs));
+        X1[o] = (T)Bx_rhs; mx[1] = fmaxf(mx[1], fabsf((float)Bx_rhs));
+    }
+    if (j >= 1 && j < N - 1) {
+        const int64_t o = (int64_t)i * ldn + (j - 1);
+        X2[o] = (T)Ex_rhs; mx[2] = fmaxf(mx[2], fabsf((float)Ex_rhs));
+        X3[o] = (T)By_rhs; mx[3] = fmaxf(mx[3], fabsf((float)By_rhs));
+    }
+    double djx_dy = 0, djy_dx = 0;
+    if (inner) {
+        djx_dy = s_jx[li][lj + 1] - s_jx[li][lj - 1];
+        djy_dx = s_jy[li + 1][lj] - s_jy[li - 1][lj];
+    }
+    const double bz_rhs = -(djx_dy - djy_dx) / h2;
+    X6[(int64_t)i * ldN + j] = (T)bz_rhs;
+    mx[6] = fmaxf(mx[6], fabsf((float)bz_rhs));
+    if (inner) {
+        const int64_t o = (int64_t)(i - 1) * ldn + (j - 1);
+        const double djx_dx = s_jx[li + 1][lj] - s_jx[li - 1][lj];
+        const double djy_dy = s_jy[li][lj + 1] - s_jy[li][lj - 1];
+        const double ez_rhs = -(djx_dx + djy_dy) / h2;
+        X4[o] = (T)ez_rhs;
+        mx[4] = fmaxf(mx[4], fabsf((float)ez_rhs));
+        if (a.with_phi) {
+            const double phi_rhs = psum(a.ro_f, a.n_f, plane, t) - psum(a.jz_f, a.n_f, plane, t);
+            X5[o] = (T)phi_rhs;
+            mx[5] = fmaxf(mx[5], fabsf((float)phi_rhs));
+        }
+    }
+}
+
+template <typename T>
 __global__ void __launch_bounds__(RHS_TX * RHS_TY)
 k_fields_rhs(RhsArgs a, T *X0, T *X1, T *X2, T *X3, T *X4, T *X5, T *X6)
 {
     __shared__ double s_ro[RHS_TY + 2][RHS_TX + 2], s_jz[RHS_TY + 2][RHS_TX + 2];
     __shared__ double s_jx[RHS_TY + 2][RHS_TX + 2], s_jy[RHS_TY + 2][RHS_TX + 2];
-    const int N = a.N, n = N - 2;
-    const int ldN = ld2(N), ldn = ld2(n);
+    const int N = a.N;
     const int64_t plane = (int64_t)N * N;
     const int i0 = blockIdx.y * RHS_TY - 1, j0 = blockIdx.x * RHS_TX - 1;
     if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0 && a.bz_sum)
         *a.bz_sum = 0.0;
+
     const int tid = threadIdx.y * RHS_TX + threadIdx.x;
     for (int e = tid; e < (RHS_TY + 2) * (RHS_TX + 2); e += RHS_TX * RHS_TY) {
         const int li = e / (RHS_TX + 2), lj = e % (RHS_TX + 2);
@@ -541,46 +981,25 @@ k_fields_rhs(RhsArgs a, T *X0, T *X1, T *X2, T *X3, T *X4, T *X5, T *X6)
     __syncthreads();
     const int li = threadIdx.y + 1, lj = threadIdx.x + 1;
     const int i = i0 + li, j = j0 + lj;
-    if (i >= N || j >= N) return;
-    const int64_t t = (int64_t)i * N + j;
-    const bool inner = i >= 1 && i < N - 1 && j >= 1 && j < N - 1;
-    const double h2 = a.h * 2;
-    double dro_dx = 0, dro_dy = 0, djz_dx = 0, djz_dy = 0;
-    if (inner) {
-        dro_dx = (s_ro[li + 1][lj] - s_ro[li - 1][lj]) / h2;
-        dro_dy = (s_ro[li][lj + 1] - s_ro[li][lj - 1]) / h2;
-        djz_dx = (s_jz[li + 1][lj] - s_jz[li - 1][lj]) / h2;
-        djz_dy = (s_jz[li][lj + 1] - s_jz[li][lj - 1]) / h2;
-    }
-    const double djx_dxi = (psum(a.jx_p, a.n_p, plane, t) - s_jx[li][lj]) / a.dxi;
-    const double djy_dxi = (psum(a.jy_p, a.n_p, plane, t) - s_jy[li][lj]) / a.dxi;
-    const double Ex_rhs = -(dro_dx - djx_dxi - a.c * a.Ex[t]);
-    const double Ey_rhs = -(dro_dy - djy_dxi - a.c * a.Ey[t]);
-    const double Bx_rhs = +(djz_dy - djy_dxi + a.c * a.Bx[t]);
-    const double By_rhs = -(djz_dx - djx_dxi - a.c * a.By[t]);
-    if (i >= 1 && i < N - 1) {
-        const int64_t o = (int64_t)(i - 1) * ldN + j;
-        X0[o] = (T)Ey_rhs;
-        X1[o] = (T)Bx_rhs;
-    }
-    if (j >= 1 && j < N - 1) {
-        const int64_t o = (int64_t)i * ldn + (j - 1);
-        X2[o] = (T)Ex_rhs;
-        X3[o] = (T)By_rhs;
-    }
-    double djx_dy = 0, djy_dx = 0;
-    if (inner) {
-        djx_dy = s_jx[li][lj + 1] - s_jx[li][lj - 1];
-        djy_dx = s_jy[li + 1][lj] - s_jy[li - 1][lj];
-    }
-    X6[(int64_t)i * ldN + j] = (T)(-(djx_dy - djy_dx) / h2);
-    if (inner) {
-        const int64_t o = (int64_t)(i - 1) * ldn + (j - 1);
-        const double djx_dx = s_jx[li + 1][lj] - s_jx[li - 1][lj];
-        const double djy_dy = s_jy[li][lj + 1] - s_jy[li][lj - 1];
-        X4[o] = (T)(-(djx_dx + djy_dy) / h2);
-        if (a.with_phi)
-            X5[o] = (T)(psum(a.ro_f, a.n_f, plane, t) - psum(a.jz_f, a.n_f, plane, t));
+    float mx[NPROB] = {0, 0, 0, 0, 0, 0, 0};
+    if (i < N && j < N) rhs_node(a, s_ro, s_jz, s_jx, s_jy, li, lj, i, j, X0, X1, X2, X3, X4, X5, X6, mx);
+    if (a.amax_out) {
+        // per-block maxima first: one atomic per block and problem
+        __shared__ float s_mx[RHS_TY][NPROB];
+#pragma unroll
+        for (int p = 0; p < NPROB; p++) {
+            float v = mx[p];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+            if (threadIdx.x == 0) s_mx[threadIdx.y][p] = v;
+        }
+        __syncthreads();
+        if (threadIdx.y == 0 && threadIdx.x < NPROB) {
+            float v = 0.f;
+#pragma unroll
+            for (int y = 0; y < RHS_TY; y++) v = fmaxf(v, s_mx[y][threadIdx.x]);
+            if (v > 0.f) atomicMax(a.amax_out + threadIdx.x, __float_as_uint(v));
+        }
     }
 }
 
@@ -630,14 +1049,23 @@ template <typename T>
 struct Work {
     T *S1[NPROB], *S2[NPROB];
     double *bz_raw, *bz_sum;
+    unsigned *amax[2];    // per-problem operand maxima, alternating between folds
 };
 
-static size_t slot_elems(int N) { return ((size_t)N * (N + 4) + 31) / 32 * 32; }
+// A workspace slot holds one problem's matrix: FP64 or FP32 rows of up to
+// N + 4 elements, or in mixed precision four int8 slice planes of rows of
+// up to N + 30 bytes (two 16-byte padded blocks per row).
+template <typename T>
+static size_t slot_elems(int N)
+{
+    const size_t w = sizeof(T) == sizeof(float) ? N + 32 : N + 4;
+    return ((size_t)N * w + 31) / 32 * 32;
+}
 
 template <typename T>
 static size_t work_bytes(int N)
 {
-    size_t b = 2 * NPROB * slot_elems(N) * sizeof(T);
+    size_t b = 2 * NPROB * slot_elems<T>(N) * sizeof(T);
     b = (b + 255) / 256 * 256;
     b += (size_t)N * N * sizeof(double);
     b = (b + 255) / 256 * 256;
@@ -650,15 +1078,18 @@ static Work<T> carve(void *ws, int N)
 {
     Work<T> w;
     T *p = static_cast<T *>(ws);
-    for (int i = 0; i < NPROB; i++) { w.S1[i] = p; p += slot_elems(N); }
-    for (int i = 0; i < NPROB; i++) { w.S2[i] = p; p += slot_elems(N); }
-    size_t off = 2 * NPROB * slot_elems(N) * sizeof(T);
+    for (int i = 0; i < NPROB; i++) { w.S1[i] = p; p += slot_elems<T>(N); }
+    for (int i = 0; i < NPROB; i++) { w.S2[i] = p; p += slot_elems<T>(N); }
+    size_t off = 2 * NPROB * slot_elems<T>(N) * sizeof(T);
     off = (off + 255) / 256 * 256;
     char *base = static_cast<char *>(ws);
     w.bz_raw = reinterpret_cast<double *>(base + off);
     off += (size_t)N * N * sizeof(double);
     off = (off + 255) / 256 * 256;
     w.bz_sum = reinterpret_cast<double *>(base + off);
+    // the last 256 bytes: bz_sum, then two arrays of NPROB maxima
+    w.amax[0] = reinterpret_cast<unsigned *>(base + off + 64);
+    w.amax[1] = reinterpret_cast<unsigned *>(base + off + 128);
     return w;
 }
 
@@ -692,13 +1123,19 @@ template <int EPI>
 static int launch_f32(const GemmBatch<float> &b, int nsub, int maxM, int maxN, int N,
                       cudaStream_t st)
 {
-    if (N > 200) {
-        dim3 grid((maxN + 63) / 64, (maxM + 63) / 64, nsub);
-        k_gemm_f32<64, 64, 16, 4, 4, EPI><<<grid, 256, 0, st>>>(b);
-    } else {
-        dim3 grid((maxN + 31) / 32, (maxM + 31) / 32, nsub);
-        k_gemm_f32<32, 32, 16, 2, 2, EPI><<<grid, 256, 0, st>>>(b);
+    constexpr int BN = 64;
+    using Cfg = I8Cfg<BN>;
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k_gemm_i8<BN, EPI>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)Cfg::smem);
+        if (e != cudaSuccess) return cuda_check(e, "i8 gemm smem attribute");
+        attr = true;
     }
+    (void)N;
+    dim3 grid((maxN + BN - 1) / BN, (maxM + I8_BM - 1) / I8_BM, nsub);
+    k_gemm_i8<BN, EPI><<<grid, 128, Cfg::smem, st>>>(b);
     return LCB_OK;
 }
 
@@ -735,7 +1172,8 @@ static int run_wave(const GemmBatch<T> &b, int nsub, int epi, int N, cudaStream_
 
 template <typename T>
 static int run_fold(T *const *src, T *const *dst, const int *probs, int np, const int *rows,
-                    const int *cols, int by_rows, int N, cudaStream_t st)
+                    const int *cols, int by_rows, int N, cudaStream_t st,
+                    const unsigned *src_max = nullptr, unsigned *clear = nullptr)
 {
     FoldBatch<T> fb;
     memset(&fb, 0, sizeof(fb));
@@ -746,6 +1184,16 @@ static int run_fold(T *const *src, T *const *dst, const int *probs, int np, cons
         fb.d[q].R = rows[p];
         fb.d[q].C = cols[p];
         fb.d[q].by_rows = by_rows;
+        fb.d[q].src_max = src_max ? src_max + p : nullptr;
+    }
+    fb.clear = clear;
+    if constexpr (sizeof(T) == sizeof(float)) {
+        if (src_max) {
+            dim3 grid((unsigned)((N / 4 + 2 + 127) / 128), (unsigned)N, np);
+            k_fold_slices<<<grid, 128, 0, st>>>(fb);
+            LCB_LAUNCH_CHECK("k_fold_slices");
+            return LCB_OK;
+        }
     }
     dim3 grid((unsigned)((N + 255) / 256), (unsigned)N, np);
     k_fold<T><<<grid, 256, 0, st>>>(fb);
@@ -757,7 +1205,7 @@ template <typename T>
 static int solve(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st)
 {
     const int N = a->grid_steps, n = N - 2;
-    const OpLayout L = op_layout(N);
+    const OpLayout L = op_layout(N, sizeof(T) == sizeof(float));
     Work<T> w = carve<T>(a->workspace, N);
     // Phi (problem 5) is skipped when neither of its outputs is wanted.
     const bool with_phi = a->out_half.f[6] || a->out_full.f[6];
@@ -776,6 +1224,18 @@ static int solve(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st
     r.Bx = a->fields.f[3]; r.By = a->fields.f[4];
     r.bz_sum = w.bz_sum;
     r.with_phi = with_phi;
+    // mixed precision: every producer of a matrix that a fold turns into
+    // int8 slices (the right-hand sides, waves 1-3) records its largest
+    // element per problem; the maxima alternate between two arrays, each
+    // fold clearing the one that the next wave fills
+    constexpr bool rec = sizeof(T) == sizeof(float);
+    unsigned *const mx0 = rec ? w.amax[0] : nullptr, *const mx1 = rec ? w.amax[1] : nullptr;
+    unsigned *cur_mx = nullptr;
+    r.amax_out = mx0;
+    if (rec) {
+        cudaError_t e = cudaMemsetAsync(mx0, 0, NPROB * sizeof(unsigned), st);
+        if (e != cudaSuccess) return cuda_check(e, "clear maxima");
+    }
     {
         dim3 grid((N + RHS_TX - 1) / RHS_TX, (N + RHS_TY - 1) / RHS_TY);
         k_fields_rhs<T><<<grid, dim3(RHS_TX, RHS_TY), 0, st>>>(
@@ -815,6 +1275,15 @@ static int solve(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st
                 d.M = rows[p]; d.K = par ? ho : he; d.N = par ? ho : he;
                 d.rmul = 1; d.radd = 0; d.cmul = 2; d.cadd = par;
                 d.C = w.S1[p]; d.ldc = ld2(C); d.prob = p;
+                d.amax_a = cur_mx ? cur_mx + p : nullptr;
+                if (rec) {
+                    // slice planes: U block, then V block (bytes)
+                    const uint8_t *base = reinterpret_cast<const uint8_t *>(w.S2[p]);
+                    d.lda = ld16(par ? ho : he);
+                    d.A = reinterpret_cast<const T *>(base + (par ? 4 * (int64_t)rows[p] * ld16(he) : 0));
+                    d.a_plane = rows[p] * d.lda;
+                    d.b_plane = (int)(L.rows[id] * L.ld[id]);
+                }
             }
         }
         return s;
@@ -836,6 +1305,14 @@ static int solve(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st
                 if (!to_fields) { d.C = w.S1[p]; d.ldc = ld2(cols[p]); }
                 d.E = op(mat[p]); d.lde = (int)L.ld[mat[p]];
                 d.prob = p;
+                d.amax_b = cur_mx ? cur_mx + p : nullptr;
+                if (rec) {
+                    const uint8_t *base = reinterpret_cast<const uint8_t *>(w.S2[p]);
+                    d.ldb = ld16(cols[p]);
+                    d.B = reinterpret_cast<const T *>(base + (par ? 4 * (int64_t)he * d.ldb : 0));
+                    d.b_plane = (par ? ho : he) * d.ldb;
+                    d.a_plane = (int)(L.rows[id] * L.ld[id]);
+                }
             }
         }
         return s;
@@ -843,16 +1320,24 @@ static int solve(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st
 
     int rc;
     // wave 1: S1 = S1 R
-    if ((rc = run_fold<T>(w.S1, w.S2, probs, np, rows, cols, 0, N, st))) return rc;
+    if ((rc = run_fold<T>(w.S1, w.S2, probs, np, rows, cols, 0, N, st, mx0, mx1))) return rc;
+    cur_mx = mx0;
+    b.amax_out = mx1;
     if ((rc = run_wave<T>(b, right_wave(), EPI_STORE, N, st, "wave1"))) return rc;
     // wave 2: S1 = (L S1) o Mat
-    if ((rc = run_fold<T>(w.S1, w.S2, probs, np, rows, cols, 1, N, st))) return rc;
+    if ((rc = run_fold<T>(w.S1, w.S2, probs, np, rows, cols, 1, N, st, mx1, mx0))) return rc;
+    cur_mx = mx1;
+    b.amax_out = mx0;
     if ((rc = run_wave<T>(b, left_wave(false), EPI_SCALE, N, st, "wave2"))) return rc;
     // wave 3: S1 = S1 R
-    if ((rc = run_fold<T>(w.S1, w.S2, probs, np, rows, cols, 0, N, st))) return rc;
+    if ((rc = run_fold<T>(w.S1, w.S2, probs, np, rows, cols, 0, N, st, mx0, mx1))) return rc;
+    cur_mx = mx0;
+    b.amax_out = mx1;
     if ((rc = run_wave<T>(b, right_wave(), EPI_STORE, N, st, "wave3"))) return rc;
     // wave 4: fields = L S1
-    if ((rc = run_fold<T>(w.S1, w.S2, probs, np, rows, cols, 1, N, st))) return rc;
+    if ((rc = run_fold<T>(w.S1, w.S2, probs, np, rows, cols, 1, N, st, mx1, mx0))) return rc;
+    cur_mx = mx1;
+    b.amax_out = nullptr;
     const int nsub = left_wave(true);
     // field index in lcb_fields: Ex 0, Ey 1, Ez 2, Bx 3, By 4, Bz 5, Phi 6
     const int fidx[NPROB] = {1, 3, 0, 4, 2, 6, 5};
@@ -895,7 +1380,7 @@ extern "C" size_t lcb_field_operators_bytes(int grid_steps, int precision)
 {
     if (grid_steps < 5 || (grid_steps % 2) == 0) return 0;
     const size_t el = precision == LCB_PREC_MIXED ? sizeof(float) : sizeof(double);
-    return (size_t)op_layout(grid_steps).off[OP_COUNT] * el;
+    return (size_t)op_layout(grid_steps, precision == LCB_PREC_MIXED).off[OP_COUNT] * el;
 }
 
 extern "C" int lcb_field_operators_build(int grid_steps, double h, double subtraction_coeff,
@@ -910,12 +1395,18 @@ extern "C" int lcb_field_operators_build(int grid_steps, double h, double subtra
                 lcb_field_operators_bytes(N, precision));
     LCB_REQUIRE(((uintptr_t)operators & 255) == 0, "operator buffer must be 256-byte aligned");
     LCB_REQUIRE(h > 0, "transverse step must be > 0");
-    const OpLayout L = op_layout(N);
+    const OpLayout L = op_layout(N, precision == LCB_PREC_MIXED);
     const int blocks = (int)((L.off[OP_COUNT] + 255) / 256);
-    if (precision == LCB_PREC_MIXED)
+    if (precision == LCB_PREC_MIXED) {
         k_build_ops<float><<<blocks, 256, 0, as_stream(stream)>>>(
             N, h, subtraction_coeff, L, static_cast<float *>(operators));
-    else
+        LCB_LAUNCH_CHECK("k_build_ops");
+        // then the transform blocks are overwritten with their slice planes
+        k_build_slices<<<(int)((L.off[OP_D] + 255) / 256), 256, 0, as_stream(stream)>>>(
+            N, L, static_cast<uint8_t *>(operators));
+        LCB_LAUNCH_CHECK("k_build_slices");
+        return LCB_OK;
+    } else
         k_build_ops<double><<<blocks, 256, 0, as_stream(stream)>>>(
             N, h, subtraction_coeff, L, static_cast<double *>(operators));
     LCB_LAUNCH_CHECK("k_build_ops");
@@ -1000,7 +1491,7 @@ extern "C" int lcb_compute_fields_noalloc(const lcb_compute_fields_args *a, void
     LCB_REQUIRE(need <= LCB_NOALLOC_FIELDS_SCRATCH_BYTES,
                 "grid_steps %d in precision %d needs %zu bytes of scratch; the "
                 "allocation-free entry point has %zu (largest grid: 261 in FP64, "
-                "359 in mixed precision) -- use lcb_compute_fields with a workspace",
+                "347 in mixed precision) -- use lcb_compute_fields with a workspace",
                 a->grid_steps, a->precision, need, (size_t)LCB_NOALLOC_FIELDS_SCRATCH_BYTES);
     void *scratch = nullptr;
     int rc = scratch_address(&scratch);

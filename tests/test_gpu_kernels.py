@@ -343,14 +343,15 @@ def test_beam_move_vs_oracle():
     assert lost.size > 0 and moved.size > 0 and fell.size > 0
 
 
-def _op_layout(N):
+def _op_layout(N, mixed=False):
     n = N - 2
     se, so, ce, co = (n + 1) // 2, (n - 1) // 2, (N + 1) // 2, (N - 1) // 2
     shapes = [(se, se), (so, so), (se, se), (so, so), (ce, ce), (co, co), (ce, ce), (co, co),
               (n, n), (n, N), (N, n), (N, N)]
     offs, lds, o = [], [], 0
     for i, (r, c) in enumerate(shapes):
-        ld = (c + 1) // 2 * 2 if i < 8 else c   # transform blocks: even row stride
+        # transform blocks: even row stride (FP64), or 16-byte rows of int8 slice planes
+        ld = ((c + 15) // 16 * 16 if mixed else (c + 1) // 2 * 2) if i < 8 else c
         offs.append(o)
         lds.append(ld)
         o += (r * ld + 31) // 32 * 32
@@ -375,8 +376,18 @@ def test_field_operators_build(N, mixed):
     blocks += cb + [cb[0].T, cb[1].T]
     blocks += [O.dirichlet_matrix(N, h), O.mixed_matrix(N, h, c), O.mixed_matrix(N, h, c).T,
                O.neumann_matrix(N, h)]
-    shapes, offs, lds = _op_layout(N)
+    shapes, offs, lds = _op_layout(N, mixed)
     rel = 1e-6 if mixed else 1e-13
+    raw = ops.buf.cpu().numpy().view(np.uint8)
     for i, (ref, shp, off, ld) in enumerate(zip(blocks, shapes, offs, lds)):
-        got = buf[off:off + shp[0] * ld].reshape(shp[0], ld)[:, :shp[1]].astype(np.float64)
-        close(got, ref, rel, f"operator block {i}")
+        if mixed and i < 8:
+            # four int8 slice planes, x = 2 sum_i s_i 2^-(6 + 7 i)
+            plane = shp[0] * ld
+            planes = [raw[4 * off + k * plane:4 * off + (k + 1) * plane].view(np.int8)
+                      .reshape(shp[0], ld)[:, :shp[1]].astype(np.float64) for k in range(4)]
+            got = 2 * sum(p * 2.0 ** -(6 + 7 * k) for k, p in enumerate(planes))
+            rel_b = 2.0 ** -23  # FP32 rounding of the value, then exact slices
+        else:
+            got = buf[off:off + shp[0] * ld].reshape(shp[0], ld)[:, :shp[1]]
+            rel_b = rel
+        close(got.astype(np.float64), ref, rel_b, f"operator block {i}")
