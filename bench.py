@@ -653,6 +653,29 @@ def main():
         dist.destroy_process_group()
 
 
+# DRAM bytes (read + written) per call of the dominant op, from one ncu
+# capture of the small case of the same workload (N=513, 11 xi steps):
+# compute_fields in FP64 counts its four DMMA waves, move_deposit the fused
+# kernel of a non-first stage.
+NCU_TRAFFIC = {("compute_fields", "fp64"): 77.8e6, ("move_deposit", "mixed"): 116.0e6}
+
+
+def transform_flops(N):
+    """Flops of the dense transforms of one compute_fields call: four waves
+    of even/odd folded products (2 M K N each) over the seven problems, Phi
+    counted in one call of two (the predictor does not need it)."""
+    n = N - 2
+    rows = [n, n, N, N, n, n, N]
+    cols = [N, N, n, n, n, n, N]
+    tot = 0.0
+    for p in range(7):
+        R, C = rows[p], cols[p]
+        right = 2 * R * (((C + 1) // 2) ** 2 + ((C - 1) // 2) ** 2)
+        left = 2 * C * (((R + 1) // 2) ** 2 + ((R - 1) // 2) ** 2)
+        tot += (0.5 if p == 5 else 1.0) * 2 * (right + left)
+    return tot
+
+
 def roofline(r, N, hbm_peak, peak_src, peaks):
     """Roofline of the dominant operation over the timed region."""
     ops = r["ops"]
@@ -662,18 +685,24 @@ def roofline(r, N, hbm_peak, peak_src, peaks):
     o = ops[name]
     Np = 964 * 964
     if name == "compute_fields":
-        # 4 waves x 7 problems, each 2*M*N*K; roughly 56 N^3 flops per call
-        flops = 56.0 * N ** 3
-        achieved = flops / (o["ms_avg"] / 1e3) / 1e12
-        peak = 37.0 if r.get("precision", "fp64") == "fp64" else peaks.get("bf16_tflops", 1590.0)
-        return {"bound": "fp64-simt", "kernel": name, "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
-                "peak_source": "nominal B200 FP64 (no measured FP64 peak)"}
+        flops = transform_flops(N)
+        if r.get("precision", "fp64") == "fp64":
+            achieved = flops / (o["ms_avg"] / 1e3) / 1e12
+            return {"bound": "tensor", "kernel": name + " (FP64 DMMA waves)", "achieved": achieved,
+                    "peak": 37.0, "unit": "TFLOP/s", "frac": achieved / 37.0,
+                    "traffic": NCU_TRAFFIC.get((name, "fp64")),
+                    "peak_source": "nominal B200 FP64 tensor (no measured FP64 peak on this pool)"}
+        # mixed: ten int8 slice products per FP32 product
+        achieved = 10 * flops / (o["ms_avg"] / 1e3) / 1e12
+        return {"bound": "tensor", "kernel": name + " (int8 tcgen05 waves)", "achieved": achieved,
+                "peak": 4500.0, "unit": "TOP/s", "frac": achieved / 4500.0, "traffic": None,
+                "peak_source": "nominal B200 dense int8 (no measured int8 peak on this pool)"}
     per = {"deposit": 72, "move_smart": 128, "move_wo_fields": 64,
            "move_deposit": 128 + 72}.get(name, 0)
     achieved = per * Np / (o["ms_avg"] / 1e3) / 1e9
     return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm_peak,
-            "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+            "unit": "GB/s", "frac": achieved / hbm_peak,
+            "traffic": NCU_TRAFFIC.get((name, r.get("precision", "fp64"))),
             "peak_source": peak_src}
 
 
