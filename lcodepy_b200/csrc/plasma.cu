@@ -659,18 +659,40 @@ __device__ __forceinline__ void gather_one(const float *sf, const double *const 
     }
 }
 
+// The shared-memory window keeps each fixed-point sum as two 32-bit words,
+// because 32-bit integer atomics are native in shared memory and 64-bit ones
+// are not: a contribution c (in units of 2^-32) adds its low 20 bits to an
+// unsigned word and c >> 20 to a signed word; the flush recombines
+// (hi << 20) + lo exactly.  A block adds at most 2 x 256 contributions to a
+// cell, so the low word stays below 2^29 and, with |c| < 2^41 (particles
+// whose scaled values reach 2^42, i.e. |value| / h^2 >= 1024, take the
+// global 64-bit path instead), the high word below 2^30.
+constexpr double FIX_SHARED_LIMIT = 4398046511104.0;   // 2^42, on values scaled by 2^32 / h^2
+
+__device__ __forceinline__ void shared_fix_add(unsigned *lo, int *hi, int idx, fix_t c)
+{
+    atomicAdd(lo + idx, (unsigned)c & 0xFFFFFu);
+    const int h = (int)((long long)c >> 20);
+    if (h) atomicAdd(hi + idx, h);
+}
+
+__device__ __forceinline__ bool shared_fix_ok(const double sv[4])
+{
+    return fmax(fmax(fabs(sv[0]), fabs(sv[1])), fmax(fabs(sv[2]), fabs(sv[3]))) < FIX_SHARED_LIMIT;
+}
+
 // Deposit of one particle's scaled values (FP64 weights, fixed-point sums).
 template <int WX, int WY>
-__device__ __forceinline__ void deposit_fix_one(fix_t *sw, fix_t *const *g, int N, int wx0,
-                                                int wy0, int cx, int cy, double xl, double yl,
-                                                const double sv[4])
+__device__ __forceinline__ void deposit_fix_one(unsigned *swl, int *swh, fix_t *const *g, int N,
+                                                int wx0, int wy0, int cx, int cy, double xl,
+                                                double yl, const double sv[4])
 {
     constexpr int WSZ = WX * WY;
     double wx[5], wy[5];
     weights4(xl, wx);
     weights4(yl, wy);
     const int lx = cx - 2 - wx0, ly = cy - 2 - wy0;
-    if (lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY) {
+    if (lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY && shared_fix_ok(sv)) {
 #pragma unroll
         for (int a = 0; a < 5; a++) {
 #pragma unroll
@@ -679,7 +701,7 @@ __device__ __forceinline__ void deposit_fix_one(fix_t *sw, fix_t *const *g, int 
                 const int c = (lx + a) * WY + ly + b;
 #pragma unroll
                 for (int q = 0; q < 4; q++)
-                    atomicAdd(sw + q * WSZ + c, fix_bits(fma(sv[q], w, FIX_MAGIC)));
+                    shared_fix_add(swl, swh, q * WSZ + c, fix_bits(fma(sv[q], w, FIX_MAGIC)));
             }
         }
     } else {
@@ -722,6 +744,8 @@ k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, d
     constexpr int FS = FieldStride<WY>::v, FSZ = WX * FS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     fix_t *sw = reinterpret_cast<fix_t *>(smem_raw);           // [4][WX][WY] deposit
+    unsigned *swl = reinterpret_cast<unsigned *>(sw);          //   as [4][WX][WY] low words
+    int *swh = reinterpret_cast<int *>(swl + 4 * WSZ);         //   and [4][WX][WY] high words
     float *sf = reinterpret_cast<float *>(sw + 4 * WSZ);       // [6][WX][FS] fields
     const int s = blockIdx.z;
     const int64_t base = (int64_t)s * n_per_sort;
@@ -924,7 +948,8 @@ k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, d
     {
         const int lx = cx[0] - 2 - wx0, ly = cy[0] - 2 - wy0;
         const bool joint = cx[0] >= 0 && cx[0] == cx[1] && cy[0] == cy[1] &&
-                           lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY;
+                           lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY &&
+                           shared_fix_ok(sv[0]) && shared_fix_ok(sv[1]);
         if (joint) {
             double ax[5], ay[5], bx[5], by[5];
             weights4(dxl[0], ax); weights4(dyl[0], ay);
@@ -937,15 +962,15 @@ k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, d
                     const int c = (lx + a) * WY + ly + b;
 #pragma unroll
                     for (int q = 0; q < 4; q++)
-                        atomicAdd(sw + q * WSZ + c,
-                                  fix_bits(fma(sv[0][q], wa, fma(sv[1][q], wb, FIX_MAGIC))));
+                        shared_fix_add(swl, swh, q * WSZ + c,
+                                       fix_bits(fma(sv[0][q], wa, fma(sv[1][q], wb, FIX_MAGIC))));
                 }
             }
         } else {
             if (cx[0] >= 0)
-                deposit_fix_one<WX, WY>(sw, g4, N, wx0, wy0, cx[0], cy[0], dxl[0], dyl[0], sv[0]);
+                deposit_fix_one<WX, WY>(swl, swh, g4, N, wx0, wy0, cx[0], cy[0], dxl[0], dyl[0], sv[0]);
             if (cx[1] >= 0)
-                deposit_fix_one<WX, WY>(sw, g4, N, wx0, wy0, cx[1], cy[1], dxl[1], dyl[1], sv[1]);
+                deposit_fix_one<WX, WY>(swl, swh, g4, N, wx0, wy0, cx[1], cy[1], dxl[1], dyl[1], sv[1]);
         }
     }
     __syncthreads();
@@ -955,8 +980,8 @@ k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, d
         const int64_t c = (int64_t)gx * N + gy;
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            const fix_t v = sw[q * WSZ + t];
-            if (v) atomicAdd(g4[q] + c, v);
+            const long long v = ((long long)swh[q * WSZ + t] << 20) + (long long)swl[q * WSZ + t];
+            if (v) atomicAdd(g4[q] + c, (fix_t)v);
         }
     }
 }
