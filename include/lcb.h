@@ -194,7 +194,7 @@ size_t lcb_compute_fields_workspace_bytes(int grid_steps, int precision);
  * every GPU that loads the library until the process exits.  Grids whose
  * scratch need (lcb_compute_fields_workspace_bytes) exceeds it are rejected
  * with LCB_ERR_INVALID; every odd grid_steps up to 261 fits in
- * LCB_PREC_FP64 and up to 347 in LCB_PREC_MIXED.  Nothing is allocated or
+ * LCB_PREC_FP64 and up to 277 in LCB_PREC_MIXED.  Nothing is allocated or
  * freed.
  *
  * The first call on a device looks up the array's device address there

@@ -89,10 +89,38 @@ struct OpLayout {
     int64_t rows[OP_COUNT], cols[OP_COUNT], ld[OP_COUNT];
 };
 
-// Transform blocks: FP64 rows padded to an even length (16-byte cp.async
-// chunks); in mixed precision four int8 slice planes of rows x ld16(cols)
-// bytes each, i.e. rows x ld16(cols) FP32 words of storage.
 __host__ __device__ constexpr int ld16(int c) { return (c + 15) & ~15; }
+
+// ---------------------------------------------------------------------------
+// Mixed precision operand storage: four int8 slice planes per matrix, each
+// plane cut into the tiles the tensor-core GEMM streams (zero padded), each
+// tile stored in the tensor cores' no-swizzle core-matrix order so that one
+// contiguous bulk copy fills a shared-memory stage.
+//   A role (M x K, K-major): 128 x 32 tiles of 4096 bytes, tile (mt, kt) at
+//     (mt KT + kt) 4096, element (r, k) at (r/8) 256 + (k/16) 128 + (r%8) 16 + k%16;
+//   B role (K x N, N-major): 32 x 64 tiles of 2048 bytes, tile (kt, nt) at
+//     (nt KT + kt) 2048, element (k, n) at (n/16) 512 + (k/8) 128 + (k%8) 16 + n%16.
+// ---------------------------------------------------------------------------
+constexpr int TL_M = 128, TL_K = 32, TL_N = 64;
+__host__ __device__ constexpr int ntiles(int x, int t) { return (x + t - 1) / t; }
+__host__ __device__ constexpr int64_t a_plane_bytes(int M, int K)
+{
+    return (int64_t)ntiles(M, TL_M) * ntiles(K, TL_K) * (TL_M * TL_K);
+}
+__host__ __device__ constexpr int64_t b_plane_bytes(int K, int N)
+{
+    return (int64_t)ntiles(K, TL_K) * ntiles(N, TL_N) * (TL_K * TL_N);
+}
+__host__ __device__ inline int64_t a_tile_off(int r, int k, int KT)
+{
+    return ((int64_t)((r >> 7) * KT + (k >> 5)) << 12) + ((r & 127) >> 3) * 256 +
+           ((k & 31) >> 4) * 128 + (r & 7) * 16 + (k & 15);
+}
+__host__ __device__ inline int64_t b_tile_off(int k, int n, int KT)
+{
+    return ((int64_t)((n >> 6) * KT + (k >> 5)) << 11) + ((n & 63) >> 4) * 512 +
+           ((k & 31) >> 3) * 128 + (k & 7) * 16 + (n & 15);
+}
 
 static OpLayout op_layout(int N, bool mixed = false)
 {
@@ -107,8 +135,14 @@ static OpLayout op_layout(int N, bool mixed = false)
         L.rows[i] = r[i];
         L.cols[i] = c[i];
         // transform blocks feed cp.async; solver matrices are read elementwise
-        L.ld[i] = i < OP_D ? (mixed ? ld16((int)c[i]) : ld2((int)c[i])) : c[i];
-        o += (r[i] * L.ld[i] + 31) / 32 * 32;
+        L.ld[i] = i < OP_D ? (mixed ? c[i] : ld2((int)c[i])) : c[i];
+        // mixed transform blocks: four tiled slice planes, A role for the
+        // left operators (SE SO CE CO), B role for the right ones (transposed)
+        const bool a_role = i == OP_SE || i == OP_SO || i == OP_CE || i == OP_CO;
+        const int64_t words = (i < OP_D && mixed)
+            ? (a_role ? a_plane_bytes((int)r[i], (int)c[i]) : b_plane_bytes((int)r[i], (int)c[i]))
+            : r[i] * L.ld[i];
+        o += (words + 31) / 32 * 32;
     }
     L.off[OP_COUNT] = o;
     return L;
@@ -169,36 +203,42 @@ __global__ void k_build_ops(int N, double h, double c, OpLayout L, T *buf)
     }
 }
 
-// Mixed precision: the transform blocks as four int8 slice planes (bound 2).
+// Mixed precision: the transform blocks as four tiled int8 slice planes
+// (bound 2); the thread of padded element e writes its four slices.
 __global__ void k_build_slices(int N, OpLayout L, uint8_t *bytes)
 {
     const int n = N - 2;
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < L.off[OP_D];
-         e += (int64_t)gridDim.x * blockDim.x) {
-        int b = 0;
-        while (b < OP_D - 1 && e >= L.off[b + 1]) b++;
-        const int64_t loc = e - L.off[b];
-        const int64_t plane = L.rows[b] * L.ld[b];
-        if (loc >= plane) continue;          // alignment padding of the block
-        const int r = (int)(loc / L.ld[b]), q = (int)(loc % L.ld[b]);
-        double v = 0;
-        if (q < L.cols[b]) {
-            switch (b) {
-            case OP_SE: v = dst1(2 * r, q, n); break;
-            case OP_SO: v = dst1(2 * r + 1, q, n); break;
-            case OP_SET: v = dst1(2 * q, r, n); break;
-            case OP_SOT: v = dst1(2 * q + 1, r, n); break;
-            case OP_CE: v = dct1(2 * r, q, N); break;
-            case OP_CO: v = dct1(2 * r + 1, q, N); break;
-            case OP_CET: v = dct1(2 * q, r, N); break;
-            case OP_COT: v = dct1(2 * q + 1, r, N); break;
-            }
-        }
-        unsigned sl[4];
-        slice4((float)v, 0.5f, sl);
+    for (int b = 0; b < OP_D; b++) {
+        const bool a_role = b == OP_SE || b == OP_SO || b == OP_CE || b == OP_CO;
+        const int R = (int)L.rows[b], C = (int)L.cols[b];
+        const int64_t plane = a_role ? a_plane_bytes(R, C) : b_plane_bytes(R, C);
+        // padded extents: A role 128-row x 32-col tiles, B role 32 x 64
+        const int Rp = a_role ? ntiles(R, TL_M) * TL_M : ntiles(R, TL_K) * TL_K;
+        const int Cp = a_role ? ntiles(C, TL_K) * TL_K : ntiles(C, TL_N) * TL_N;
+        const int KT = a_role ? ntiles(C, TL_K) : ntiles(R, TL_K);
         uint8_t *base = bytes + 4 * L.off[b];
+        for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < (int64_t)Rp * Cp;
+             e += (int64_t)gridDim.x * blockDim.x) {
+            const int r = (int)(e / Cp), q = (int)(e % Cp);
+            double v = 0;
+            if (r < R && q < C) {
+                switch (b) {
+                case OP_SE: v = dst1(2 * r, q, n); break;
+                case OP_SO: v = dst1(2 * r + 1, q, n); break;
+                case OP_SET: v = dst1(2 * q, r, n); break;
+                case OP_SOT: v = dst1(2 * q + 1, r, n); break;
+                case OP_CE: v = dct1(2 * r, q, N); break;
+                case OP_CO: v = dct1(2 * r + 1, q, N); break;
+                case OP_CET: v = dct1(2 * q, r, N); break;
+                case OP_COT: v = dct1(2 * q + 1, r, N); break;
+                }
+            }
+            unsigned sl[4];
+            slice4((float)v, 0.5f, sl);
+            const int64_t at = a_role ? a_tile_off(r, q, KT) : b_tile_off(r, q, KT);
 #pragma unroll
-        for (int i = 0; i < 4; i++) base[i * plane + loc] = (uint8_t)sl[i];
+            for (int i = 0; i < 4; i++) base[i * plane + at] = (uint8_t)sl[i];
+        }
     }
 }
 
@@ -219,8 +259,8 @@ struct GemmDesc {
     // by the fold pass that produced it); NULL for a transform block, whose
     // elements are bounded by 2
     const unsigned *amax_a, *amax_b;
-    // mixed precision: A and B are four int8 slice planes; lda / ldb are then
-    // row strides in bytes and a_plane / b_plane the plane strides in bytes
+    // mixed precision: A and B are four tiled int8 slice planes (A role and
+    // B role); a_plane / b_plane are the plane strides in bytes
     int a_plane, b_plane;
 };
 
@@ -546,24 +586,33 @@ __device__ __forceinline__ double epi_apply(const GemmBatch<float> &b, const Gem
 
 template <int BN>
 struct I8Cfg {
+    static_assert(BN == TL_N, "B tiles are 64 wide");
     static constexpr int ST = 4;                                       // pipeline stages
     static constexpr int B_SLICE = I8_BK * BN;                         // bytes
     static constexpr int STAGE = I8_NS * (I8_A_SLICE + B_SLICE);       // bytes
     static constexpr int TMEM_COLS = 4 * BN;                           // power of two
-    static constexpr size_t smem = (size_t)ST * STAGE + 64;
+    static constexpr size_t smem = (size_t)ST * STAGE + 128;   // + 2 ST + 1 barriers, TMEM slot
 };
 
+__device__ __forceinline__ void bulk_g2s(unsigned dst, const void *src, unsigned bytes, unsigned mbar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                 :: "r"(dst), "l"(src), "r"(bytes), "r"(mbar) : "memory");
+}
+
 template <int BN, int EPI>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(256)
 k_gemm_i8(const __grid_constant__ GemmBatch<float> batch)
 {
     using Cfg = I8Cfg<BN>;
     constexpr int ST = Cfg::ST;
     static_assert(Cfg::TMEM_COLS == 256 || Cfg::TMEM_COLS == 512, "tensor memory columns");
-    static_assert(4 * 32 * (BN + 1) * sizeof(float) <= (size_t)ST * Cfg::STAGE, "epilogue staging");
+    static_assert(8 * 32 * 33 * sizeof(float) <= (size_t)ST * Cfg::STAGE, "epilogue staging");
     extern __shared__ __align__(1024) uint8_t i8sm[];
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(i8sm + ST * Cfg::STAGE);   // [ST]
-    unsigned *tslot = reinterpret_cast<unsigned *>(mbar + ST);
+    uint64_t *full = reinterpret_cast<uint64_t *>(i8sm + ST * Cfg::STAGE);   // [ST] copies landed
+    uint64_t *done = full + ST;                                             // [ST] MMAs finished
+    uint64_t *fin = done + ST;                                              // all MMAs finished
+    unsigned *tslot = reinterpret_cast<unsigned *>(fin + 1);
 
     const GemmDesc<float> &g = batch.d[blockIdx.z];
     const int M = g.M, N = g.N, K = g.K;
@@ -571,8 +620,10 @@ k_gemm_i8(const __grid_constant__ GemmBatch<float> batch)
     if (m0 >= M || n0 >= N) return;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int ea = operand_exp(g.amax_a), eb = operand_exp(g.amax_b);
-    const uint8_t *Ab = reinterpret_cast<const uint8_t *>(g.A);
-    const uint8_t *Bb = reinterpret_cast<const uint8_t *>(g.B);
+    const int KT = ntiles(K, TL_K);
+    // this CTA's tile rows of A and tile column of B
+    const uint8_t *At = reinterpret_cast<const uint8_t *>(g.A) + (int64_t)blockIdx.y * KT * I8_A_SLICE;
+    const uint8_t *Bt = reinterpret_cast<const uint8_t *>(g.B) + (int64_t)blockIdx.x * KT * Cfg::B_SLICE;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -580,8 +631,8 @@ k_gemm_i8(const __grid_constant__ GemmBatch<float> batch)
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0)
-        for (int q = 0; q < ST; q++)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(mbar + q)), "r"(1)
+        for (int q = 0; q < 2 * ST + 1; q++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(full + q)), "r"(1)
                          : "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -589,55 +640,35 @@ k_gemm_i8(const __grid_constant__ GemmBatch<float> batch)
     const unsigned tmem = *tslot;
     const unsigned idesc = i8_idesc<BN>();
 
-    // one stage: A rows m0.. (K-major cores), B rows k0.. (MN-major cores),
-    // 16-byte chunks of the slice planes, zero past the matrix edges
-    auto issue = [&](int buf, int kt) {
-        uint8_t *sA = i8sm + buf * Cfg::STAGE;
-        uint8_t *sB = sA + I8_NS * I8_A_SLICE;
-        const int k0 = kt * I8_BK;
-#pragma unroll
-        for (int c = tid; c < I8_NS * I8_BM * 2; c += 128) {
-            const int sl = c / (2 * I8_BM), rem = c % (2 * I8_BM), r = rem >> 1, hk = rem & 1;
-            const int gm = m0 + r, gk = k0 + 16 * hk;
-            int bytes = gm < M ? K - gk : 0;
-            bytes = bytes < 0 ? 0 : (bytes > 16 ? 16 : bytes);
-            const uint8_t *src = bytes ? Ab + (int64_t)sl * g.a_plane + (int64_t)gm * g.lda + gk : Ab;
-            cp_async16(sA + sl * I8_A_SLICE + (r >> 3) * 256 + hk * 128 + (r & 7) * 16, src, bytes);
-        }
-#pragma unroll
-        for (int c = tid; c < I8_NS * I8_BK * (BN / 16); c += 128) {
-            const int sl = c / (I8_BK * (BN / 16)), rem = c % (I8_BK * (BN / 16));
-            const int kr = rem % I8_BK, nc = rem / I8_BK;
-            const int gk = k0 + kr, gn = n0 + 16 * nc;
-            int bytes = gk < K ? N - gn : 0;
-            bytes = bytes < 0 ? 0 : (bytes > 16 ? 16 : bytes);
-            const uint8_t *src = bytes ? Bb + (int64_t)sl * g.b_plane + (int64_t)gk * g.ldb + gn : Bb;
-            cp_async16(sB + sl * Cfg::B_SLICE + nc * 512 + (kr >> 3) * 128 + (kr & 7) * 16, src,
-                       bytes);
-        }
-    };
-
-    // loads run PF stages ahead; a buffer is refilled ST - PF stages after its
-    // MMAs were issued, so neither the copies nor the MMAs are waited on
-    // right after they start
-    constexpr int PF = 2;
-    static_assert(PF >= 1 && PF < ST, "pipeline depth");
-    const int nk = (K + I8_BK - 1) / I8_BK;
-#pragma unroll
-    for (int q = 0; q < PF; q++) {
-        if (q < nk) issue(q, q);
-        cp_async_commit();
-    }
     bool ok = true;
-    for (int kt = 0; kt < nk; kt++) {
-        const int buf = kt % ST;
-        cp_async_wait<PF - 1>();
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
+    if (warp == 0) {
+        // warp 0 streams the stages (eight bulk copies each: four A and four
+        // B slice tiles) and issues the MMAs from lane 0; the whole warp
+        // follows the loop so that lane 0 never diverges from idle lanes
+        auto load = [&](int kt) {
+            if (lane != 0) return;
+            const int buf = kt % ST;
+            const unsigned sA = smem_u32(i8sm + buf * Cfg::STAGE);
+            const unsigned sB = sA + I8_NS * I8_A_SLICE;
+            const unsigned mb = smem_u32(full + buf);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;"
+                         :: "r"((unsigned)Cfg::STAGE), "r"(mb) : "memory");
+#pragma unroll
+            for (int i = 0; i < I8_NS; i++) {
+                bulk_g2s(sA + i * I8_A_SLICE, At + (int64_t)i * g.a_plane + (int64_t)kt * I8_A_SLICE,
+                         I8_A_SLICE, mb);
+                bulk_g2s(sB + i * Cfg::B_SLICE, Bt + (int64_t)i * g.b_plane + (int64_t)kt * Cfg::B_SLICE,
+                         Cfg::B_SLICE, mb);
+            }
+        };
+        for (int kt = 0; kt < ST && kt < KT; kt++) load(kt);
+        for (int kt = 0; kt < KT; kt++) {
+            const int buf = kt % ST;
+            ok &= mbar_wait(smem_u32(full + buf), (kt / ST) & 1);
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const unsigned a0 = smem_u32(i8sm + buf * Cfg::STAGE);
             const unsigned b0 = a0 + I8_NS * I8_A_SLICE;
+            if (lane == 0) {
 #pragma unroll
             for (int i = 0; i < I8_NS; i++) {
 #pragma unroll
@@ -654,32 +685,39 @@ k_gemm_i8(const __grid_constant__ GemmBatch<float> batch)
                 }
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                         :: "r"(smem_u32(mbar + buf)) : "memory");
+                         :: "r"(smem_u32(done + buf)) : "memory");
+            if (kt == KT - 1)
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                             :: "r"(smem_u32(fin)) : "memory");
+            }
+            __syncwarp();
+            // refill the buffer of stage kt - 1 (its MMAs were issued a stage ago)
+            const int nxt = kt - 1 + ST;
+            if (kt >= 1 && nxt < KT) {
+                ok &= mbar_wait(smem_u32(done + (kt - 1) % ST), ((kt - 1) / ST) & 1);
+                load(nxt);
+            }
         }
-        // refill the buffer of stage nxt - ST once its MMAs are done
-        const int nxt = kt + PF;
-        if (nxt < nk) {
-            if (nxt >= ST) ok &= mbar_wait(smem_u32(mbar + (nxt - ST) % ST), ((nxt - ST) / ST) & 1);
-            issue(nxt % ST, nxt);
-        }
-        cp_async_commit();
     }
-    // the last commit covers every MMA issued before it
-    ok &= mbar_wait(smem_u32(mbar + (nk - 1) % ST), ((nk - 1) / ST) & 1);
-    cp_async_wait<0>();
+    // every thread waits for the one-time barrier of the last commit, which
+    // covers all MMAs (the stage barriers complete several phases each)
+    ok &= mbar_wait(smem_u32(fin), 0);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
-    // epilogue: warp w holds rows 32 w .. 32 w + 31 of the tile (its TMEM
-    // lanes); the combined values go through shared memory (the pipeline
-    // buffers are free now) so that the stores run along rows
-    float *stage = reinterpret_cast<float *>(i8sm) + warp * 32 * (BN + 1);
-    const double scale = ldexp(1.0, ea + eb - 12);
+    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (tile rows) and
+    // columns 32 (w / 4) .. + 31; the four accumulators combine exactly in
+    // 64-bit integers (a0 2^21 + a1 2^14 + a2 2^7 + a3, |.| < 2^53) with one
+    // conversion per element; the values go through shared memory (the
+    // pipeline buffers are free now) so that the stores run along rows
+    const int rq = warp & 3, ch = warp >> 2;
+    float *stage = reinterpret_cast<float *>(i8sm) + warp * 32 * 33;
+    const float scale = ldexpf(1.f, ea + eb - 33);
 #pragma unroll 1
-    for (int c8 = 0; c8 < BN / 8; c8++) {
+    for (int c8 = 0; c8 < 4; c8++) {
         unsigned r[4][8];
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            const unsigned taddr = tmem + ((unsigned)(32 * warp) << 16) + (unsigned)(q * BN + 8 * c8);
+            const unsigned taddr = tmem + ((unsigned)(32 * rq) << 16) + (unsigned)(q * BN + 32 * ch + 8 * c8);
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                          : "=r"(r[q][0]), "=r"(r[q][1]), "=r"(r[q][2]), "=r"(r[q][3]),
                            "=r"(r[q][4]), "=r"(r[q][5]), "=r"(r[q][6]), "=r"(r[q][7])
@@ -688,9 +726,10 @@ k_gemm_i8(const __grid_constant__ GemmBatch<float> batch)
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
         for (int e = 0; e < 8; e++) {
-            const double d = (double)(int)r[0][e] + ldexp((double)(int)r[1][e], -7) +
-                             ldexp((double)(int)r[2][e], -14) + ldexp((double)(int)r[3][e], -21);
-            stage[lane * (BN + 1) + 8 * c8 + e] = ok ? (float)(d * scale) : __int_as_float(0x7fc00000);
+            const long long c = ((long long)(int)r[0][e] << 21) + ((long long)(int)r[1][e] << 14) +
+                                ((long long)(int)r[2][e] << 7) + (long long)(int)r[3][e];
+            // x = c 2^(ea + eb - 33): exact up to the one rounding to FP32
+            stage[lane * 33 + 8 * c8 + e] = ok ? (float)c * scale : __int_as_float(0x7fc00000);
         }
     }
     __syncwarp();
@@ -698,26 +737,20 @@ k_gemm_i8(const __grid_constant__ GemmBatch<float> batch)
     float vmax = 0.f;
     // rows in groups of 8: the scale factors or previous fields they need
     // are loaded for the whole group before any store
-    constexpr int CB = BN / 32;
 #pragma unroll 1
     for (int r0 = 0; r0 < 32; r0 += 8) {
-        double pre[8][CB];
+        double pre[8];
 #pragma unroll
-        for (int rr = 0; rr < 8; rr++)
+        for (int rr = 0; rr < 8; rr++) {
+            const int gm = m0 + 32 * rq + r0 + rr, gn = n0 + 32 * ch + lane;
+            pre[rr] = (gm < M && gn < N) ? epi_pre<EPI>(batch, g, gm, gn) : 0.0;
+        }
 #pragma unroll
-            for (int cb = 0; cb < CB; cb++) {
-                const int gm = m0 + 32 * warp + r0 + rr, gn = n0 + 32 * cb + lane;
-                pre[rr][cb] = (gm < M && gn < N) ? epi_pre<EPI>(batch, g, gm, gn) : 0.0;
-            }
-#pragma unroll
-        for (int rr = 0; rr < 8; rr++)
-#pragma unroll
-            for (int cb = 0; cb < CB; cb++) {
-                const int gm = m0 + 32 * warp + r0 + rr, col = 32 * cb + lane, gn = n0 + col;
-                if (gm >= M || gn >= N) continue;
-                const float v = stage[(r0 + rr) * (BN + 1) + col];
-                part += epi_apply<EPI>(batch, g, gm, gn, v, pre[rr][cb], vmax);
-            }
+        for (int rr = 0; rr < 8; rr++) {
+            const int gm = m0 + 32 * rq + r0 + rr, gn = n0 + 32 * ch + lane;
+            if (gm >= M || gn >= N) continue;
+            part += epi_apply<EPI>(batch, g, gm, gn, stage[(r0 + rr) * 33 + lane], pre[rr], vmax);
+        }
     }
     if (EPI != EPI_FIELD && batch.amax_out) {
 #pragma unroll
@@ -729,7 +762,7 @@ k_gemm_i8(const __grid_constant__ GemmBatch<float> batch)
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
                      :: "r"(tmem), "r"(Cfg::TMEM_COLS) : "memory");
-    if (EPI == EPI_FIELD && batch.out[g.prob].kind == 3) bz_reduce<128>(part, batch.out[g.prob].bz_sum);
+    if (EPI == EPI_FIELD && batch.out[g.prob].kind == 3) bz_reduce<256>(part, batch.out[g.prob].bz_sum);
 }
 
 // ---------------------------------------------------------------------------
@@ -755,8 +788,12 @@ struct FoldBatch {
     unsigned *clear;      // NPROB maxima zeroed here for the next producer, or NULL
 };
 
-// Mixed precision fold: FP32 source, int8 slice planes out.  A thread makes
-// four consecutive outputs of a row, one 32-bit store per plane.
+// Mixed precision fold: FP32 source, tiled int8 slice planes out (zero
+// padded).  Column folds feed right waves, so U (R x he) and V (R x ho) are
+// stored in the A role; row folds feed left waves, so U (he x C) and V
+// (ho x C) are stored in the B role.  A thread makes four consecutive
+// elements along the contiguous direction of a core-matrix row (K for A,
+// N for B): one 32-bit store per plane.
 __device__ __forceinline__ void put_slices4(uint8_t *blk, int64_t plane, int64_t at,
                                             const float v[4], float scale)
 {
@@ -780,51 +817,52 @@ __global__ void __launch_bounds__(128) k_fold_slices(const __grid_constant__ Fol
         fb.clear[threadIdx.x] = 0u;
     const float scale = ldexpf(1.f, -bound_exp(2.f * __uint_as_float(*f.src_max)));
     uint8_t *blk = reinterpret_cast<uint8_t *>(f.dst);
-    for (int i = blockIdx.y; i < R; i += gridDim.y) {
-        if (!f.by_rows) {
-            const int he = (C + 1) / 2, ho = C - he, mid = (C - 1) / 2;
-            const int gu = (he + 3) / 4, gv = (ho + 3) / 4;
-            const float *row = f.src + (int64_t)i * ldc;
-            for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < gu + gv;
-                 t += gridDim.x * blockDim.x) {
-                float v[4];
-                if (t < gu) {
-#pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        const int j = 4 * t + e;
-                        v[e] = j < mid ? row[j] + row[C - 1 - j] : (j == mid ? row[mid] : 0.f);
-                    }
-                    put_slices4(blk, (int64_t)R * ld16(he), (int64_t)i * ld16(he) + 4 * t, v, scale);
-                } else {
-                    const int tv = t - gu;
-#pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        const int jj = 4 * tv + e;
-                        v[e] = jj < ho ? row[jj] - row[C - 1 - jj] : 0.f;
-                    }
-                    put_slices4(blk + 4 * (int64_t)R * ld16(he), (int64_t)R * ld16(ho),
-                                (int64_t)i * ld16(ho) + 4 * tv, v, scale);
-                }
-            }
-        } else {
-            const int he = (R + 1) / 2, ho = R - he, mid = (R - 1) / 2;
-            const int64_t ldb = ld16(C);
-            const float *ra = f.src + (int64_t)(i < he ? i : i - he) * ldc;
-            const float *rb = f.src + (int64_t)(i < he ? R - 1 - i : R - 1 - (i - he)) * ldc;
-            const bool single = i == mid && i < he;
-            for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < (C + 3) / 4;
-                 t += gridDim.x * blockDim.x) {
+    if (!f.by_rows) {
+        const int he = (C + 1) / 2, ho = C - he, mid = (C - 1) / 2;
+        const int Rp = ntiles(R, TL_M) * TL_M;
+        const int KTu = ntiles(he, TL_K), KTv = ntiles(ho, TL_K);
+        const int64_t pu = a_plane_bytes(R, he), pv = a_plane_bytes(R, ho);
+        for (int y = blockIdx.y; y < 2 * Rp; y += gridDim.y) {
+            const bool isv = y >= Rp;
+            const int r = isv ? y - Rp : y;
+            const int KT = isv ? KTv : KTu, groups = KT * TL_K / 4;
+            const float *row = f.src + (int64_t)(r < R ? r : 0) * ldc;
+            for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < groups; t += gridDim.x * blockDim.x) {
                 float v[4];
 #pragma unroll
                 for (int e = 0; e < 4; e++) {
                     const int j = 4 * t + e;
-                    v[e] = j >= C ? 0.f : (single ? ra[j] : (i < he ? ra[j] + rb[j] : ra[j] - rb[j]));
+                    if (r >= R) v[e] = 0.f;
+                    else if (!isv) v[e] = j < mid ? row[j] + row[C - 1 - j] : (j == mid ? row[mid] : 0.f);
+                    else v[e] = j < ho ? row[j] - row[C - 1 - j] : 0.f;
                 }
-                if (i < he)
-                    put_slices4(blk, (int64_t)he * ldb, (int64_t)i * ldb + 4 * t, v, scale);
-                else
-                    put_slices4(blk + 4 * (int64_t)he * ldb, (int64_t)ho * ldb,
-                                (int64_t)(i - he) * ldb + 4 * t, v, scale);
+                if (!isv) put_slices4(blk, pu, a_tile_off(r, 4 * t, KTu), v, scale);
+                else put_slices4(blk + 4 * pu, pv, a_tile_off(r, 4 * t, KTv), v, scale);
+            }
+        }
+    } else {
+        const int he = (R + 1) / 2, ho = R - he, mid = (R - 1) / 2;
+        const int KTu = ntiles(he, TL_K), KTv = ntiles(ho, TL_K);
+        const int Kpu = KTu * TL_K, Kpv = KTv * TL_K;
+        const int groups = ntiles(C, TL_N) * TL_N / 4;
+        const int64_t pu = b_plane_bytes(he, C), pv = b_plane_bytes(ho, C);
+        for (int y = blockIdx.y; y < Kpu + Kpv; y += gridDim.y) {
+            const bool isv = y >= Kpu;
+            const int k = isv ? y - Kpu : y;
+            const bool valid = isv ? k < ho : k < he;
+            const float *ra = f.src + (int64_t)(valid ? k : 0) * ldc;
+            const float *rb = f.src + (int64_t)(valid ? R - 1 - k : 0) * ldc;
+            const bool single = !isv && k == mid;
+            for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < groups; t += gridDim.x * blockDim.x) {
+                float v[4];
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const int n = 4 * t + e;
+                    v[e] = (!valid || n >= C) ? 0.f
+                         : (single ? ra[n] : (isv ? ra[n] - rb[n] : ra[n] + rb[n]));
+                }
+                if (!isv) put_slices4(blk, pu, b_tile_off(k, 4 * t, KTu), v, scale);
+                else put_slices4(blk + 4 * pu, pv, b_tile_off(k, 4 * t, KTv), v, scale);
             }
         }
     }
@@ -1053,13 +1091,15 @@ struct Work {
 };
 
 // A workspace slot holds one problem's matrix: FP64 or FP32 rows of up to
-// N + 4 elements, or in mixed precision four int8 slice planes of rows of
-// up to N + 30 bytes (two 16-byte padded blocks per row).
+// N + 4 elements, or in mixed precision the four tiled int8 slice planes of
+// a folded matrix.
 template <typename T>
 static size_t slot_elems(int N)
 {
-    const size_t w = sizeof(T) == sizeof(float) ? N + 32 : N + 4;
-    return ((size_t)N * w + 31) / 32 * 32;
+    // mixed: four tiled slice planes of both fold halves, at most
+    // (N + 127) x (N + 64) bytes each, i.e. that many FP32 words
+    const size_t e = sizeof(T) == sizeof(float) ? (size_t)(N + 128) * (N + 64) : (size_t)N * (N + 4);
+    return (e + 31) / 32 * 32;
 }
 
 template <typename T>
@@ -1135,7 +1175,7 @@ static int launch_f32(const GemmBatch<float> &b, int nsub, int maxM, int maxN, i
     }
     (void)N;
     dim3 grid((maxN + BN - 1) / BN, (maxM + I8_BM - 1) / I8_BM, nsub);
-    k_gemm_i8<BN, EPI><<<grid, 128, Cfg::smem, st>>>(b);
+    k_gemm_i8<BN, EPI><<<grid, 256, Cfg::smem, st>>>(b);
     return LCB_OK;
 }
 
@@ -1189,7 +1229,10 @@ static int run_fold(T *const *src, T *const *dst, const int *probs, int np, cons
     fb.clear = clear;
     if constexpr (sizeof(T) == sizeof(float)) {
         if (src_max) {
-            dim3 grid((unsigned)((N / 4 + 2 + 127) / 128), (unsigned)N, np);
+            // rows: up to 2 x 128-padded rows (column fold); columns: up to
+            // (N + 64) / 4 groups of four
+            dim3 grid((unsigned)(((N + TL_N) / 4 + 127) / 128),
+                      (unsigned)(2 * ntiles(N, TL_M) * TL_M), np);
             k_fold_slices<<<grid, 128, 0, st>>>(fb);
             LCB_LAUNCH_CHECK("k_fold_slices");
             return LCB_OK;
@@ -1277,12 +1320,11 @@ static int solve(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st
                 d.C = w.S1[p]; d.ldc = ld2(C); d.prob = p;
                 d.amax_a = cur_mx ? cur_mx + p : nullptr;
                 if (rec) {
-                    // slice planes: U block, then V block (bytes)
+                    // tiled slice planes (A role): U block, then V block
                     const uint8_t *base = reinterpret_cast<const uint8_t *>(w.S2[p]);
-                    d.lda = ld16(par ? ho : he);
-                    d.A = reinterpret_cast<const T *>(base + (par ? 4 * (int64_t)rows[p] * ld16(he) : 0));
-                    d.a_plane = rows[p] * d.lda;
-                    d.b_plane = (int)(L.rows[id] * L.ld[id]);
+                    d.A = reinterpret_cast<const T *>(base + (par ? 4 * a_plane_bytes(rows[p], he) : 0));
+                    d.a_plane = (int)a_plane_bytes(rows[p], d.K);
+                    d.b_plane = (int)b_plane_bytes((int)L.rows[id], (int)L.cols[id]);
                 }
             }
         }
@@ -1307,11 +1349,11 @@ static int solve(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st
                 d.prob = p;
                 d.amax_b = cur_mx ? cur_mx + p : nullptr;
                 if (rec) {
+                    // tiled slice planes (B role): U block, then V block
                     const uint8_t *base = reinterpret_cast<const uint8_t *>(w.S2[p]);
-                    d.ldb = ld16(cols[p]);
-                    d.B = reinterpret_cast<const T *>(base + (par ? 4 * (int64_t)he * d.ldb : 0));
-                    d.b_plane = (par ? ho : he) * d.ldb;
-                    d.a_plane = (int)(L.rows[id] * L.ld[id]);
+                    d.B = reinterpret_cast<const T *>(base + (par ? 4 * b_plane_bytes(he, cols[p]) : 0));
+                    d.b_plane = (int)b_plane_bytes(d.K, cols[p]);
+                    d.a_plane = (int)a_plane_bytes((int)L.rows[id], (int)L.cols[id]);
                 }
             }
         }
@@ -1491,7 +1533,7 @@ extern "C" int lcb_compute_fields_noalloc(const lcb_compute_fields_args *a, void
     LCB_REQUIRE(need <= LCB_NOALLOC_FIELDS_SCRATCH_BYTES,
                 "grid_steps %d in precision %d needs %zu bytes of scratch; the "
                 "allocation-free entry point has %zu (largest grid: 261 in FP64, "
-                "347 in mixed precision) -- use lcb_compute_fields with a workspace",
+                "277 in mixed precision) -- use lcb_compute_fields with a workspace",
                 a->grid_steps, a->precision, need, (size_t)LCB_NOALLOC_FIELDS_SCRATCH_BYTES);
     void *scratch = nullptr;
     int rc = scratch_address(&scratch);

@@ -350,12 +350,39 @@ def _op_layout(N, mixed=False):
               (n, n), (n, N), (N, n), (N, N)]
     offs, lds, o = [], [], 0
     for i, (r, c) in enumerate(shapes):
-        # transform blocks: even row stride (FP64), or 16-byte rows of int8 slice planes
-        ld = ((c + 15) // 16 * 16 if mixed else (c + 1) // 2 * 2) if i < 8 else c
+        # transform blocks: even row stride (FP64), or four tiled int8 slice planes
+        ld = c if (mixed or i >= 8) else (c + 1) // 2 * 2
         offs.append(o)
         lds.append(ld)
-        o += (r * ld + 31) // 32 * 32
+        words = _plane_bytes(i, r, c) if (mixed and i < 8) else r * ld
+        o += (words + 31) // 32 * 32
     return shapes, offs, lds
+
+
+def _tiles(x, t):
+    return (x + t - 1) // t
+
+
+def _a_role(i):
+    return i in (0, 1, 4, 5)   # SE SO CE CO: left operators
+
+
+def _plane_bytes(i, r, c):
+    if _a_role(i):
+        return _tiles(r, 128) * _tiles(c, 32) * 4096
+    return _tiles(r, 32) * _tiles(c, 64) * 2048
+
+
+def _tile_offsets(i, r, c):
+    """Byte offset of every element (row, col) of a tiled slice plane."""
+    R, Cc = np.meshgrid(np.arange(r), np.arange(c), indexing="ij")
+    if _a_role(i):
+        KT = _tiles(c, 32)
+        return (((R >> 7) * KT + (Cc >> 5)) << 12) + ((R & 127) >> 3) * 256 + \
+            ((Cc & 31) >> 4) * 128 + (R & 7) * 16 + (Cc & 15)
+    KT = _tiles(r, 32)
+    return (((Cc >> 6) * KT + (R >> 5)) << 11) + ((Cc & 63) >> 4) * 512 + \
+        ((R & 31) >> 3) * 128 + (R & 7) * 16 + (Cc & 15)
 
 
 @pytest.mark.parametrize("N,mixed", [(33, False), (129, False), (65, True)])
@@ -381,10 +408,11 @@ def test_field_operators_build(N, mixed):
     raw = ops.buf.cpu().numpy().view(np.uint8)
     for i, (ref, shp, off, ld) in enumerate(zip(blocks, shapes, offs, lds)):
         if mixed and i < 8:
-            # four int8 slice planes, x = 2 sum_i s_i 2^-(6 + 7 i)
-            plane = shp[0] * ld
-            planes = [raw[4 * off + k * plane:4 * off + (k + 1) * plane].view(np.int8)
-                      .reshape(shp[0], ld)[:, :shp[1]].astype(np.float64) for k in range(4)]
+            # four tiled int8 slice planes, x = 2 sum_k s_k 2^-(6 + 7 k)
+            plane = _plane_bytes(i, *shp)
+            at = _tile_offsets(i, *shp)
+            planes = [raw[4 * off + k * plane:4 * off + (k + 1) * plane].view(np.int8)[at]
+                      .astype(np.float64) for k in range(4)]
             got = 2 * sum(p * 2.0 ** -(6 + 7 * k) for k, p in enumerate(planes))
             rel_b = 2.0 ** -23  # FP32 rounding of the value, then exact slices
         else:
