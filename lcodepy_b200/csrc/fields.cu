@@ -809,12 +809,16 @@ __device__ __forceinline__ void put_slices4(uint8_t *blk, int64_t plane, int64_t
     for (int i = 0; i < 4; i++) *reinterpret_cast<unsigned *>(blk + i * plane + at) = w[i];
 }
 
+// Block: 32 x 4 threads, four output rows (threadIdx.y) with 32 threads
+// striding over each row's groups of four.
 __global__ void __launch_bounds__(128) k_fold_slices(const __grid_constant__ FoldBatch<float> fb)
 {
     const FoldDesc<float> &f = fb.d[blockIdx.z];
     const int R = f.R, C = f.C, ldc = ld2(C);
-    if (fb.clear && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x < NPROB)
+    if (fb.clear && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.y == 0 &&
+        threadIdx.x < NPROB)
         fb.clear[threadIdx.x] = 0u;
+    const int row0 = blockIdx.y * blockDim.y + threadIdx.y, rstep = gridDim.y * blockDim.y;
     const float scale = ldexpf(1.f, -bound_exp(2.f * __uint_as_float(*f.src_max)));
     uint8_t *blk = reinterpret_cast<uint8_t *>(f.dst);
     if (!f.by_rows) {
@@ -822,12 +826,12 @@ __global__ void __launch_bounds__(128) k_fold_slices(const __grid_constant__ Fol
         const int Rp = ntiles(R, TL_M) * TL_M;
         const int KTu = ntiles(he, TL_K), KTv = ntiles(ho, TL_K);
         const int64_t pu = a_plane_bytes(R, he), pv = a_plane_bytes(R, ho);
-        for (int y = blockIdx.y; y < 2 * Rp; y += gridDim.y) {
+        for (int y = row0; y < 2 * Rp; y += rstep) {
             const bool isv = y >= Rp;
             const int r = isv ? y - Rp : y;
             const int KT = isv ? KTv : KTu, groups = KT * TL_K / 4;
             const float *row = f.src + (int64_t)(r < R ? r : 0) * ldc;
-            for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < groups; t += gridDim.x * blockDim.x) {
+            for (int t = threadIdx.x; t < groups; t += blockDim.x) {
                 float v[4];
 #pragma unroll
                 for (int e = 0; e < 4; e++) {
@@ -846,14 +850,14 @@ __global__ void __launch_bounds__(128) k_fold_slices(const __grid_constant__ Fol
         const int Kpu = KTu * TL_K, Kpv = KTv * TL_K;
         const int groups = ntiles(C, TL_N) * TL_N / 4;
         const int64_t pu = b_plane_bytes(he, C), pv = b_plane_bytes(ho, C);
-        for (int y = blockIdx.y; y < Kpu + Kpv; y += gridDim.y) {
+        for (int y = row0; y < Kpu + Kpv; y += rstep) {
             const bool isv = y >= Kpu;
             const int k = isv ? y - Kpu : y;
             const bool valid = isv ? k < ho : k < he;
             const float *ra = f.src + (int64_t)(valid ? k : 0) * ldc;
             const float *rb = f.src + (int64_t)(valid ? R - 1 - k : 0) * ldc;
             const bool single = !isv && k == mid;
-            for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < groups; t += gridDim.x * blockDim.x) {
+            for (int t = threadIdx.x; t < groups; t += blockDim.x) {
                 float v[4];
 #pragma unroll
                 for (int e = 0; e < 4; e++) {
@@ -1229,11 +1233,12 @@ static int run_fold(T *const *src, T *const *dst, const int *probs, int np, cons
     fb.clear = clear;
     if constexpr (sizeof(T) == sizeof(float)) {
         if (src_max) {
-            // rows: up to 2 x 128-padded rows (column fold); columns: up to
-            // (N + 64) / 4 groups of four
-            dim3 grid((unsigned)(((N + TL_N) / 4 + 127) / 128),
-                      (unsigned)(2 * ntiles(N, TL_M) * TL_M), np);
-            k_fold_slices<<<grid, 128, 0, st>>>(fb);
+            // output rows: 2 x 128-padded rows (column fold) or the two
+            // 32-padded halves (row fold), four per block
+            const int nrows = by_rows ? ntiles((N + 1) / 2, TL_K) * TL_K * 2
+                                      : 2 * ntiles(N, TL_M) * TL_M;
+            dim3 grid(1u, (unsigned)((nrows + 3) / 4), np);
+            k_fold_slices<<<grid, dim3(32, 4), 0, st>>>(fb);
             LCB_LAUNCH_CHECK("k_fold_slices");
             return LCB_OK;
         }
