@@ -193,8 +193,8 @@ size_t lcb_compute_fields_workspace_bytes(int grid_steps, int precision);
  * array of LCB_NOALLOC_FIELDS_SCRATCH_BYTES bytes inside liblcb.so, held on
  * every GPU that loads the library until the process exits.  Grids whose
  * scratch need (lcb_compute_fields_workspace_bytes) exceeds it are rejected
- * with LCB_ERR_INVALID; every odd grid_steps up to 261 fits in
- * LCB_PREC_FP64 and up to 277 in LCB_PREC_MIXED.  Nothing is allocated or
+ * with LCB_ERR_INVALID; every odd grid_steps up to 283 fits in
+ * LCB_PREC_FP64 and up to 427 in LCB_PREC_MIXED.  Nothing is allocated or
  * freed.
  *
  * The first call on a device looks up the array's device address there
@@ -203,7 +203,7 @@ size_t lcb_compute_fields_workspace_bytes(int grid_steps, int precision);
  * previous call's contents in it; the solver clears what must start at zero
  * itself.  Calls that overlap on the GPU (e.g. on two streams at once) race
  * on the array and give wrong results: serialise them. */
-#define LCB_NOALLOC_FIELDS_SCRATCH_BYTES ((size_t)8 << 20)
+#define LCB_NOALLOC_FIELDS_SCRATCH_BYTES ((size_t)16 << 20)
 int lcb_compute_fields_noalloc(const lcb_compute_fields_args *a, void *stream);
 
 /* ---------------------------------------------------------------------

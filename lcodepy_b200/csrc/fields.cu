@@ -25,8 +25,9 @@
 // difference block V); the products write their even/odd outputs back
 // interleaved, so every result is in natural order again.
 //
-// FP64 products run on the FP64 tensor cores (mma.sync m8n8k4 .f64); FP32
-// products (mixed precision) on the FP32 cores.
+// All products run on the int8 tensor cores (tcgen05) on sliced operands,
+// exactly: eight slices reproduce FP64 accuracy, four FP32 accuracy (mixed
+// precision).
 #include <cstring>
 
 #include "common.cuh"
@@ -45,17 +46,24 @@ enum { P_EY = 0, P_BX, P_EX, P_BY, P_EZ, P_PHI, P_BZ };
 enum { OP_SE, OP_SO, OP_SET, OP_SOT, OP_CE, OP_CO, OP_CET, OP_COT,
        OP_D, OP_MX, OP_MXT, OP_NM, OP_COUNT };
 
-// Leading dimensions of the dense operands are padded to an even number of
-// elements so that every row starts on a 16-byte boundary (cp.async chunks).
+// Leading dimension of the natural-layout matrices (right-hand sides,
+// products): padded to an even number of elements.
 __host__ __device__ constexpr int ld2(int c) { return (c + 1) & ~1; }
 
-// The four int8 slices of x * scale (|x * scale| <= 1), each as a byte in the
-// low bits: the float sum with 1.5 * 2^23 rounds to an integer held in the
-// low mantissa bits.
-__device__ __forceinline__ void slice4(float x, float scale, unsigned sl[4])
+// Operands of the tensor-core transforms are written as int8 slices,
+//     x = 2^E (s_0 2^-6 + s_1 2^-13 + ... + s_{NS-1} 2^-(6 + 7 (NS - 1))),
+// |s_i| <= 64: four slices for FP32 operands (mixed precision), eight for
+// FP64 ones.  slices_of returns the slices of x * scale (|x * scale| <= 1),
+// each as a byte in the low bits: the sum with 1.5 * 2^23 (FP32) or
+// 1.5 * 2^52 (FP64) rounds to an integer held in the low mantissa bits.
+template <int NS>
+__device__ __forceinline__ void slices_of(double x, double scale, unsigned sl[NS]);
+
+template <>
+__device__ __forceinline__ void slices_of<4>(double x, double scale, unsigned sl[4])
 {
     const float MG = 12582912.0f;
-    float u = x * scale * 64.f;
+    float u = (float)x * (float)scale * 64.f;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
         const float v = u + MG;
@@ -64,15 +72,26 @@ __device__ __forceinline__ void slice4(float x, float scale, unsigned sl[4])
     }
 }
 
-// The four slices packed in one 32-bit word, slice i in byte i: the form in
-// which the mixed-precision field solve stores transform blocks and folded
-// data (the same four bytes per element as FP32).
-__device__ __forceinline__ unsigned pack_slices(float x, float scale)
+template <>
+__device__ __forceinline__ void slices_of<8>(double x, double scale, unsigned sl[8])
 {
-    unsigned sl[4];
-    slice4(x, scale, sl);
-    return sl[0] | (sl[1] << 8) | (sl[2] << 16) | (sl[3] << 24);
+    const double MG = 6755399441055744.0;
+    double u = x * scale * 64.0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const double v = u + MG;
+        sl[i] = (unsigned)__double_as_longlong(v) & 0xFFu;
+        u = (u - (v - MG)) * 128.0;
+    }
 }
+
+// Slices per element of an operand of type T (one byte each: the sliced
+// form takes the same storage as T).
+template <typename T> struct Slices { static constexpr int n = (int)sizeof(T); };
+
+// A float upper bound of |x| (rounded up), for the per-problem maxima.
+__device__ __forceinline__ float abs_bound(float x) { return fabsf(x); }
+__device__ __forceinline__ float abs_bound(double x) { return __double2float_ru(fabs(x)); }
 
 // Exponent E with m <= 2^E for m >= 0 (0 for m = 0).
 __device__ __forceinline__ int bound_exp(float m)
@@ -89,7 +108,6 @@ struct OpLayout {
     int64_t rows[OP_COUNT], cols[OP_COUNT], ld[OP_COUNT];
 };
 
-__host__ __device__ constexpr int ld16(int c) { return (c + 15) & ~15; }
 
 // ---------------------------------------------------------------------------
 // Mixed precision operand storage: four int8 slice planes per matrix, each
@@ -122,7 +140,7 @@ __host__ __device__ inline int64_t b_tile_off(int k, int n, int KT)
            ((k & 31) >> 3) * 128 + (k & 7) * 16 + (n & 15);
 }
 
-static OpLayout op_layout(int N, bool mixed = false)
+static OpLayout op_layout(int N)
 {
     const int n = N - 2;
     const int se = (n + 1) / 2, so = (n - 1) / 2, ce = (N + 1) / 2, co = (N - 1) / 2;
@@ -134,12 +152,12 @@ static OpLayout op_layout(int N, bool mixed = false)
         L.off[i] = o;
         L.rows[i] = r[i];
         L.cols[i] = c[i];
-        // transform blocks feed cp.async; solver matrices are read elementwise
-        L.ld[i] = i < OP_D ? (mixed ? c[i] : ld2((int)c[i])) : c[i];
-        // mixed transform blocks: four tiled slice planes, A role for the
-        // left operators (SE SO CE CO), B role for the right ones (transposed)
+        L.ld[i] = c[i];
+        // transform blocks: sizeof(T) tiled slice planes (as many elements of
+        // T as one plane has bytes), A role for the left operators (SE SO CE
+        // CO), B role for the right ones (transposed); spectral matrices in T
         const bool a_role = i == OP_SE || i == OP_SO || i == OP_CE || i == OP_CO;
-        const int64_t words = (i < OP_D && mixed)
+        const int64_t words = i < OP_D
             ? (a_role ? a_plane_bytes((int)r[i], (int)c[i]) : b_plane_bytes((int)r[i], (int)c[i]))
             : r[i] * L.ld[i];
         o += (words + 31) / 32 * 32;
@@ -203,8 +221,9 @@ __global__ void k_build_ops(int N, double h, double c, OpLayout L, T *buf)
     }
 }
 
-// Mixed precision: the transform blocks as four tiled int8 slice planes
-// (bound 2); the thread of padded element e writes its four slices.
+// The transform blocks as NS tiled int8 slice planes (bound 2); the thread
+// of padded element e writes its NS slices.
+template <int NS>
 __global__ void k_build_slices(int N, OpLayout L, uint8_t *bytes)
 {
     const int n = N - 2;
@@ -216,7 +235,7 @@ __global__ void k_build_slices(int N, OpLayout L, uint8_t *bytes)
         const int Rp = a_role ? ntiles(R, TL_M) * TL_M : ntiles(R, TL_K) * TL_K;
         const int Cp = a_role ? ntiles(C, TL_K) * TL_K : ntiles(C, TL_N) * TL_N;
         const int KT = a_role ? ntiles(C, TL_K) : ntiles(R, TL_K);
-        uint8_t *base = bytes + 4 * L.off[b];
+        uint8_t *base = bytes + (int64_t)NS * L.off[b];
         for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < (int64_t)Rp * Cp;
              e += (int64_t)gridDim.x * blockDim.x) {
             const int r = (int)(e / Cp), q = (int)(e % Cp);
@@ -233,11 +252,11 @@ __global__ void k_build_slices(int N, OpLayout L, uint8_t *bytes)
                 case OP_COT: v = dct1(2 * q + 1, r, N); break;
                 }
             }
-            unsigned sl[4];
-            slice4((float)v, 0.5f, sl);
+            unsigned sl[NS];
+            slices_of<NS>(v, 0.5, sl);
             const int64_t at = a_role ? a_tile_off(r, q, KT) : b_tile_off(r, q, KT);
 #pragma unroll
-            for (int i = 0; i < 4; i++) base[i * plane + at] = (uint8_t)sl[i];
+            for (int i = 0; i < NS; i++) base[i * plane + at] = (uint8_t)sl[i];
         }
     }
 }
@@ -284,38 +303,6 @@ struct GemmBatch {
     unsigned *amax_out;   // mixed: per-problem max |stored value| (zeroed), or NULL
 };
 
-// Store one output element (m, n) of sub-product g; returns the value that
-// enters the Bz sum (0 otherwise).
-template <typename T, int EPI>
-__device__ __forceinline__ double epilogue(const GemmBatch<T> &batch, const GemmDesc<T> &g,
-                                           int m, int n, T v)
-{
-    const int om = g.rmul * m + g.radd, on = g.cmul * n + g.cadd;
-    if (EPI == EPI_STORE) {
-        g.C[(int64_t)om * g.ldc + on] = v;
-    } else if (EPI == EPI_SCALE) {
-        g.C[(int64_t)om * g.ldc + on] = v * g.E[(int64_t)om * g.lde + on];
-    } else {
-        const FieldOut &o = batch.out[g.prob];
-        const int64_t off = (int64_t)(om + o.row_off) * batch.grid_n + on + o.col_off;
-        const double dv = (double)v;
-        if (o.kind == 0) {
-            if (o.half) o.half[off] = dv;
-            if (o.full) o.full[off] = 2 * dv - o.prev[off];
-        } else if (o.kind == 1) {
-            if (o.full) o.full[off] = dv;
-            if (o.half) o.half[off] = (dv + o.prev[off]) / 2;
-        } else if (o.kind == 2) {
-            if (o.full) o.full[off] = dv;
-            if (o.half) o.half[off] = dv;
-        } else {
-            o.bz_raw[off] = dv;
-            return dv;
-        }
-    }
-    return 0.0;
-}
-
 template <int NT>
 __device__ __forceinline__ void bz_reduce(double part, double *dst)
 {
@@ -333,164 +320,34 @@ __device__ __forceinline__ void bz_reduce(double part, double *dst)
     }
 }
 
-// ---------------------------------------------------------------------------
-// cp.async helpers (16-byte chunks, zero-filled past the valid bytes).
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int bytes)
-{
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n"
-                 :: "r"(s), "l"(gmem), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" :: "n"(N) : "memory"); }
 
 // ---------------------------------------------------------------------------
-// FP64 products on the tensor cores: mma.sync.m8n8k4 .f64.  A warp owns a
-// 32 x 32 tile (4 x 4 mma tiles); the CTA is WM x WN warps.  A and B tiles
-// of depth 16 stream through an ST-stage cp.async pipeline in shared memory.
-// Fragment layouts (PTX ISA, m8n8k4 f64): A row = lane/4, col = lane%4;
-// B row = lane%4, col = lane/4; C row = lane/4, cols 2(lane%4) + {0,1}.
-// Shared-memory row strides (20 and BN + 8 doubles) make both fragment loads
-// conflict-free (two wavefronts for 256 bytes).
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b)
-{
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-                 : "+d"(c0), "+d"(c1) : "d"(a), "d"(b));
-}
-
-template <int WM, int WN, int ST>
-struct DmmaCfg {
-    static constexpr int BM = 32 * WM, BN = 32 * WN, BK = 16, NT = WM * WN * 32;
-    static constexpr int AST = BK + 4, BST = BN + 8;
-    static constexpr size_t smem = (size_t)ST * (BM * AST + BK * BST) * sizeof(double);
-};
-
-template <int WM, int WN, int ST, int EPI>
-__global__ void __launch_bounds__(WM * WN * 32)
-k_gemm_dmma(const __grid_constant__ GemmBatch<double> batch)
-{
-    using Cfg = DmmaCfg<WM, WN, ST>;
-    constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, NT = Cfg::NT;
-    constexpr int AST = Cfg::AST, BST = Cfg::BST;
-    extern __shared__ __align__(16) double dsm[];
-    double *As = dsm;                       // [ST][BM][AST]
-    double *Bs = dsm + ST * BM * AST;       // [ST][BK][BST]
-
-    const GemmDesc<double> &g = batch.d[blockIdx.z];
-    const int M = g.M, N = g.N, K = g.K;
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-    if (m0 >= M || n0 >= N) return;
-    const double *__restrict__ A = g.A;
-    const double *__restrict__ B = g.B;
-    const int lda = g.lda, ldb = g.ldb;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wm = warp / WN, wn = warp % WN;
-
-    auto issue = [&](int stage, int k0) {
-        double *as = As + stage * BM * AST;
-        double *bs = Bs + stage * BK * BST;
-#pragma unroll
-        for (int c = tid; c < BM * (BK / 2); c += NT) {
-            const int r = c / (BK / 2), cc = c % (BK / 2);
-            const int gm = m0 + r, gk = k0 + 2 * cc;
-            int bytes = (gm < M) ? (K - gk) * 8 : 0;
-            bytes = bytes < 0 ? 0 : (bytes > 16 ? 16 : bytes);
-            const double *src = bytes ? A + (int64_t)gm * lda + gk : A;
-            cp_async16(as + r * AST + 2 * cc, src, bytes);
-        }
-#pragma unroll
-        for (int c = tid; c < BK * (BN / 2); c += NT) {
-            const int r = c / (BN / 2), cc = c % (BN / 2);
-            const int gk = k0 + r, gn = n0 + 2 * cc;
-            int bytes = (gk < K) ? (N - gn) * 8 : 0;
-            bytes = bytes < 0 ? 0 : (bytes > 16 ? 16 : bytes);
-            const double *src = bytes ? B + (int64_t)gk * ldb + gn : B;
-            cp_async16(bs + r * BST + 2 * cc, src, bytes);
-        }
-    };
-
-    double acc[4][4][2];
-#pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
-
-    const int nk = (K + BK - 1) / BK;
-#pragma unroll
-    for (int s = 0; s < ST - 1; s++) {
-        if (s < nk) issue(s, s * BK);
-        cp_async_commit();
-    }
-    const int ar = wm * 32 + (lane >> 2), ac = lane & 3;
-    const int br = lane & 3, bc = wn * 32 + (lane >> 2);
-    for (int kt = 0; kt < nk; kt++) {
-        cp_async_wait<ST - 2>();
-        __syncthreads();
-        const int nxt = kt + ST - 1;
-        if (nxt < nk) issue(nxt % ST, nxt * BK);
-        cp_async_commit();
-        const double *as = As + (kt % ST) * BM * AST;
-        const double *bs = Bs + (kt % ST) * BK * BST;
-#pragma unroll
-        for (int ks = 0; ks < BK / 4; ks++) {
-            double a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) a[i] = as[(ar + 8 * i) * AST + ks * 4 + ac];
-#pragma unroll
-            for (int j = 0; j < 4; j++) b[j] = bs[(ks * 4 + br) * BST + bc + 8 * j];
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-#pragma unroll
-                for (int j = 0; j < 4; j++) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
-        }
-    }
-    cp_async_wait<0>();
-
-    double part = 0;
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const int gm = m0 + wm * 32 + 8 * i + (lane >> 2);
-        if (gm >= M) continue;
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-#pragma unroll
-            for (int t = 0; t < 2; t++) {
-                const int gn = n0 + wn * 32 + 8 * j + 2 * (lane & 3) + t;
-                if (gn < N) part += epilogue<double, EPI>(batch, g, gm, gn, acc[i][j][t]);
-            }
-        }
-    }
-    if (EPI == EPI_FIELD && batch.out[g.prob].kind == 3) bz_reduce<NT>(part, batch.out[g.prob].bz_sum);
-}
-
-// ---------------------------------------------------------------------------
-// FP32 transforms on the 5th-generation tensor cores (mixed precision),
-// exact in integer arithmetic.  Every FP32 operand element is written as
-//     x = 2^E (s0 2^-6 + s1 2^-13 + s2 2^-20 + s3 2^-27),  |s_i| <= 64,
-// with E the exponent of its matrix's largest |element| (the fold pass that
-// produced the matrix records it; transform blocks are bounded by 2), so the
-// slices are int8 and the representation error is below 2^(E-28).  The
-// product of two such matrices is the sum over slice pairs (i, j) of int8
-// GEMMs scaled by 2^-(12 + 7(i+j)); the ten pairs with i + j <= 3 go to four
-// int32 accumulators in tensor memory (one per i + j), where tcgen05.mma
-// kind::i8 sums them exactly (|sum| < 4 * 64 * 64 * K < 2^31 for K < 2^17).
-// The epilogue combines the four in FP64: the result is as accurate as an
-// FP32 product and, unlike FP32 or TF32 tensor-core accumulation, free of
-// rounding bias and independent of summation order.
+// The dense transforms on the 5th-generation tensor cores, exact in integer
+// arithmetic.  Every operand element is written as NS int8 slices,
+//     x = 2^E (s_0 2^-6 + s_1 2^-13 + ... ),  |s_i| <= 64,
+// with E the exponent of its matrix's bound (the producer of the matrix
+// records its largest element; a fold at most doubles it; transform blocks
+// are bounded by 2): NS = 4 for FP32 operands (mixed precision,
+// representation error below 2^(E-28)) and NS = 8 for FP64 ones (below
+// 2^(E-56)).  The product of two such matrices is the sum over slice pairs
+// (i, j) of int8 GEMMs scaled by 2^-(12 + 7(i+j)); the pairs with
+// i + j < NS go to NS int32 accumulators in tensor memory (one per i + j),
+// where tcgen05.mma kind::i8 sums them exactly (|sum| < NS 64^2 K < 2^31
+// for these K).  The epilogue combines them in 64-bit integers: the result
+// is as accurate as a product in the operands' precision and, unlike
+// floating-point tensor-core accumulation, free of rounding bias and
+// independent of summation order.
 //
-// CTA: 128 threads, a 128 x BN output tile in tensor memory (BN columns per
-// accumulator), K in stages of 32.  Every thread converts a share of the
-// stage's FP32 tiles into slices in shared memory (canonical no-swizzle
-// layouts: A K-major, core matrices of 8 rows x 16 bytes, 128 bytes apart
-// along K and 256 along M; B MN-major, core matrices of 8 K-rows x 16
-// bytes, 128 bytes apart along K and 512 along N); thread 0 issues the ten
-// MMAs and commits them to the stage's mbarrier, which the threads wait on
-// before refilling that stage's buffers two stages later.
+// CTA: 256 threads; a 128 x 64 output tile in tensor memory (64 columns per
+// accumulator), K in stages of 32.  The operands are stored pre-tiled (see
+// the tile geometry above), so a stage is 2 NS bulk copies issued by one
+// lane of warp 0, completing on the stage's mbarrier; the same lane issues
+// the MMAs and commits them to a second mbarrier per stage, which gates the
+// refill of that stage's buffers.  A final one-shot commit releases the
+// epilogue: all eight warps read TMEM (warp w: lanes 32 (w % 4), columns
+// 32 (w / 4)) and store through shared memory.
 // ---------------------------------------------------------------------------
-constexpr int I8_BM = 128, I8_BK = 32, I8_NS = 4;
+constexpr int I8_BM = 128, I8_BK = 32;
 constexpr int I8_A_SLICE = I8_BM * I8_BK;            // bytes per slice of the A tile
 
 __device__ __forceinline__ unsigned smem_u32(const void *p)
@@ -537,8 +394,8 @@ __device__ __forceinline__ bool mbar_wait(unsigned mbar, unsigned parity)
 
 // Epilogue of the integer products, split so that a group of outputs can
 // load what it needs (scale factor, previous field) before storing.
-template <int EPI>
-__device__ __forceinline__ double epi_pre(const GemmBatch<float> &b, const GemmDesc<float> &g,
+template <int EPI, typename T>
+__device__ __forceinline__ double epi_pre(const GemmBatch<T> &b, const GemmDesc<T> &g,
                                           int m, int n)
 {
     const int om = g.rmul * m + g.radd, on = g.cmul * n + g.cadd;
@@ -551,18 +408,18 @@ __device__ __forceinline__ double epi_pre(const GemmBatch<float> &b, const GemmD
     return 0.0;
 }
 
-template <int EPI>
-__device__ __forceinline__ double epi_apply(const GemmBatch<float> &b, const GemmDesc<float> &g,
-                                            int m, int n, float v, double pre, float &vmax)
+template <int EPI, typename T>
+__device__ __forceinline__ double epi_apply(const GemmBatch<T> &b, const GemmDesc<T> &g,
+                                            int m, int n, T v, double pre, float &vmax)
 {
     const int om = g.rmul * m + g.radd, on = g.cmul * n + g.cadd;
     if (EPI == EPI_STORE) {
         g.C[(int64_t)om * g.ldc + on] = v;
-        vmax = fmaxf(vmax, fabsf(v));
+        vmax = fmaxf(vmax, abs_bound(v));
     } else if (EPI == EPI_SCALE) {
-        const float st = v * (float)pre;
+        const T st = v * (T)pre;
         g.C[(int64_t)om * g.ldc + on] = st;
-        vmax = fmaxf(vmax, fabsf(st));
+        vmax = fmaxf(vmax, abs_bound(st));
     } else {
         const FieldOut &o = b.out[g.prob];
         const int64_t off = (int64_t)(om + o.row_off) * b.grid_n + on + o.col_off;
@@ -584,13 +441,13 @@ __device__ __forceinline__ double epi_apply(const GemmBatch<float> &b, const Gem
     return 0.0;
 }
 
-template <int BN>
+template <int NS, int BN>
 struct I8Cfg {
     static_assert(BN == TL_N, "B tiles are 64 wide");
     static constexpr int ST = 4;                                       // pipeline stages
     static constexpr int B_SLICE = I8_BK * BN;                         // bytes
-    static constexpr int STAGE = I8_NS * (I8_A_SLICE + B_SLICE);       // bytes
-    static constexpr int TMEM_COLS = 4 * BN;                           // power of two
+    static constexpr int STAGE = NS * (I8_A_SLICE + B_SLICE);          // bytes
+    static constexpr int TMEM_COLS = NS * BN;                          // power of two
     static constexpr size_t smem = (size_t)ST * STAGE + 128;   // + 2 ST + 1 barriers, TMEM slot
 };
 
@@ -600,21 +457,22 @@ __device__ __forceinline__ void bulk_g2s(unsigned dst, const void *src, unsigned
                  :: "r"(dst), "l"(src), "r"(bytes), "r"(mbar) : "memory");
 }
 
-template <int BN, int EPI>
+template <typename T, int BN, int EPI>
 __global__ void __launch_bounds__(256)
-k_gemm_i8(const __grid_constant__ GemmBatch<float> batch)
+k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
 {
-    using Cfg = I8Cfg<BN>;
+    constexpr int NS = Slices<T>::n;
+    using Cfg = I8Cfg<NS, BN>;
     constexpr int ST = Cfg::ST;
     static_assert(Cfg::TMEM_COLS == 256 || Cfg::TMEM_COLS == 512, "tensor memory columns");
-    static_assert(8 * 32 * 33 * sizeof(float) <= (size_t)ST * Cfg::STAGE, "epilogue staging");
+    static_assert(8 * 32 * 33 * sizeof(T) <= (size_t)ST * Cfg::STAGE, "epilogue staging");
     extern __shared__ __align__(1024) uint8_t i8sm[];
     uint64_t *full = reinterpret_cast<uint64_t *>(i8sm + ST * Cfg::STAGE);   // [ST] copies landed
     uint64_t *done = full + ST;                                             // [ST] MMAs finished
     uint64_t *fin = done + ST;                                              // all MMAs finished
     unsigned *tslot = reinterpret_cast<unsigned *>(fin + 1);
 
-    const GemmDesc<float> &g = batch.d[blockIdx.z];
+    const GemmDesc<T> &g = batch.d[blockIdx.z];
     const int M = g.M, N = g.N, K = g.K;
     const int m0 = blockIdx.y * I8_BM, n0 = blockIdx.x * BN;
     if (m0 >= M || n0 >= N) return;
@@ -649,12 +507,12 @@ k_gemm_i8(const __grid_constant__ GemmBatch<float> batch)
             if (lane != 0) return;
             const int buf = kt % ST;
             const unsigned sA = smem_u32(i8sm + buf * Cfg::STAGE);
-            const unsigned sB = sA + I8_NS * I8_A_SLICE;
+            const unsigned sB = sA + NS * I8_A_SLICE;
             const unsigned mb = smem_u32(full + buf);
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;"
                          :: "r"((unsigned)Cfg::STAGE), "r"(mb) : "memory");
 #pragma unroll
-            for (int i = 0; i < I8_NS; i++) {
+            for (int i = 0; i < NS; i++) {
                 bulk_g2s(sA + i * I8_A_SLICE, At + (int64_t)i * g.a_plane + (int64_t)kt * I8_A_SLICE,
                          I8_A_SLICE, mb);
                 bulk_g2s(sB + i * Cfg::B_SLICE, Bt + (int64_t)i * g.b_plane + (int64_t)kt * Cfg::B_SLICE,
@@ -667,12 +525,12 @@ k_gemm_i8(const __grid_constant__ GemmBatch<float> batch)
             ok &= mbar_wait(smem_u32(full + buf), (kt / ST) & 1);
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const unsigned a0 = smem_u32(i8sm + buf * Cfg::STAGE);
-            const unsigned b0 = a0 + I8_NS * I8_A_SLICE;
+            const unsigned b0 = a0 + NS * I8_A_SLICE;
             if (lane == 0) {
 #pragma unroll
-            for (int i = 0; i < I8_NS; i++) {
+            for (int i = 0; i < NS; i++) {
 #pragma unroll
-                for (int j = 0; j < I8_NS - i; j++) {
+                for (int j = 0; j < NS - i; j++) {
                     const uint64_t da = umma_desc(a0 + i * I8_A_SLICE, 128, 256);
                     const uint64_t db = umma_desc(b0 + j * Cfg::B_SLICE, 128, 512);
                     const unsigned acc = tmem + (unsigned)((i + j) * BN);
@@ -705,18 +563,19 @@ k_gemm_i8(const __grid_constant__ GemmBatch<float> batch)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
     // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (tile rows) and
-    // columns 32 (w / 4) .. + 31; the four accumulators combine exactly in
-    // 64-bit integers (a0 2^21 + a1 2^14 + a2 2^7 + a3, |.| < 2^53) with one
-    // conversion per element; the values go through shared memory (the
-    // pipeline buffers are free now) so that the stores run along rows
+    // columns 32 (w / 4) .. + 31; the NS accumulators combine exactly in
+    // 64-bit integers, four at a time (a0 2^21 + a1 2^14 + a2 2^7 + a3,
+    // |.| < 2^53), with one conversion per four; the values go through shared
+    // memory (the pipeline buffers are free now) so that the stores run along
+    // rows
     const int rq = warp & 3, ch = warp >> 2;
-    float *stage = reinterpret_cast<float *>(i8sm) + warp * 32 * 33;
-    const float scale = ldexpf(1.f, ea + eb - 33);
+    T *stage = reinterpret_cast<T *>(i8sm) + warp * 32 * 33;
+    const double scale = ldexp(1.0, ea + eb - 33);
 #pragma unroll 1
     for (int c8 = 0; c8 < 4; c8++) {
-        unsigned r[4][8];
+        unsigned r[NS][8];
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
+        for (int q = 0; q < NS; q++) {
             const unsigned taddr = tmem + ((unsigned)(32 * rq) << 16) + (unsigned)(q * BN + 32 * ch + 8 * c8);
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                          : "=r"(r[q][0]), "=r"(r[q][1]), "=r"(r[q][2]), "=r"(r[q][3]),
@@ -726,10 +585,18 @@ k_gemm_i8(const __grid_constant__ GemmBatch<float> batch)
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
         for (int e = 0; e < 8; e++) {
+            T v;
             const long long c = ((long long)(int)r[0][e] << 21) + ((long long)(int)r[1][e] << 14) +
                                 ((long long)(int)r[2][e] << 7) + (long long)(int)r[3][e];
-            // x = c 2^(ea + eb - 33): exact up to the one rounding to FP32
-            stage[lane * 33 + 8 * c8 + e] = ok ? (float)c * scale : __int_as_float(0x7fc00000);
+            if constexpr (NS == 4) {
+                // x = c 2^(ea + eb - 33): exact up to the one rounding to FP32
+                v = (T)((float)c * (float)scale);
+            } else {
+                const long long c2 = ((long long)(int)r[4][e] << 21) + ((long long)(int)r[5][e] << 14) +
+                                     ((long long)(int)r[6][e] << 7) + (long long)(int)r[7][e];
+                v = (T)(((double)c + ldexp((double)c2, -28)) * scale);
+            }
+            stage[lane * 33 + 8 * c8 + e] = ok ? v : (T)__int_as_float(0x7fc00000);
         }
     }
     __syncwarp();
@@ -743,13 +610,13 @@ k_gemm_i8(const __grid_constant__ GemmBatch<float> batch)
 #pragma unroll
         for (int rr = 0; rr < 8; rr++) {
             const int gm = m0 + 32 * rq + r0 + rr, gn = n0 + 32 * ch + lane;
-            pre[rr] = (gm < M && gn < N) ? epi_pre<EPI>(batch, g, gm, gn) : 0.0;
+            pre[rr] = (gm < M && gn < N) ? epi_pre<EPI, T>(batch, g, gm, gn) : 0.0;
         }
 #pragma unroll
         for (int rr = 0; rr < 8; rr++) {
             const int gm = m0 + 32 * rq + r0 + rr, gn = n0 + 32 * ch + lane;
             if (gm >= M || gn >= N) continue;
-            part += epi_apply<EPI>(batch, g, gm, gn, stage[(r0 + rr) * 33 + lane], pre[rr], vmax);
+            part += epi_apply<EPI, T>(batch, g, gm, gn, stage[(r0 + rr) * 33 + lane], pre[rr], vmax);
         }
     }
     if (EPI != EPI_FIELD && batch.amax_out) {
@@ -788,38 +655,43 @@ struct FoldBatch {
     unsigned *clear;      // NPROB maxima zeroed here for the next producer, or NULL
 };
 
-// Mixed precision fold: FP32 source, tiled int8 slice planes out (zero
-// padded).  Column folds feed right waves, so U (R x he) and V (R x ho) are
-// stored in the A role; row folds feed left waves, so U (he x C) and V
-// (ho x C) are stored in the B role.  A thread makes four consecutive
-// elements along the contiguous direction of a core-matrix row (K for A,
-// N for B): one 32-bit store per plane.
+// Slice fold: FP32 or FP64 source, tiled int8 slice planes out (zero
+// padded, sizeof(T) planes).  Column folds feed right waves, so U (R x he)
+// and V (R x ho) are stored in the A role; row folds feed left waves, so U
+// (he x C) and V (ho x C) are stored in the B role.  A thread makes four
+// consecutive elements along the contiguous direction of a core-matrix row
+// (K for A, N for B): one 32-bit store per plane.
+template <int NS, typename T>
 __device__ __forceinline__ void put_slices4(uint8_t *blk, int64_t plane, int64_t at,
-                                            const float v[4], float scale)
+                                            const T v[4], double scale)
 {
-    unsigned w[4] = {0u, 0u, 0u, 0u};
+    unsigned w[NS];
+#pragma unroll
+    for (int i = 0; i < NS; i++) w[i] = 0u;
 #pragma unroll
     for (int e = 0; e < 4; e++) {
-        unsigned sl[4];
-        slice4(v[e], scale, sl);
+        unsigned sl[NS];
+        slices_of<NS>((double)v[e], scale, sl);
 #pragma unroll
-        for (int i = 0; i < 4; i++) w[i] |= sl[i] << (8 * e);
+        for (int i = 0; i < NS; i++) w[i] |= sl[i] << (8 * e);
     }
 #pragma unroll
-    for (int i = 0; i < 4; i++) *reinterpret_cast<unsigned *>(blk + i * plane + at) = w[i];
+    for (int i = 0; i < NS; i++) *reinterpret_cast<unsigned *>(blk + i * plane + at) = w[i];
 }
 
 // Block: 32 x 4 threads, four output rows (threadIdx.y) with 32 threads
 // striding over each row's groups of four.
-__global__ void __launch_bounds__(128) k_fold_slices(const __grid_constant__ FoldBatch<float> fb)
+template <typename T>
+__global__ void __launch_bounds__(128) k_fold_slices(const __grid_constant__ FoldBatch<T> fb)
 {
-    const FoldDesc<float> &f = fb.d[blockIdx.z];
+    constexpr int NS = Slices<T>::n;
+    const FoldDesc<T> &f = fb.d[blockIdx.z];
     const int R = f.R, C = f.C, ldc = ld2(C);
     if (fb.clear && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.y == 0 &&
         threadIdx.x < NPROB)
         fb.clear[threadIdx.x] = 0u;
     const int row0 = blockIdx.y * blockDim.y + threadIdx.y, rstep = gridDim.y * blockDim.y;
-    const float scale = ldexpf(1.f, -bound_exp(2.f * __uint_as_float(*f.src_max)));
+    const double scale = ldexp(1.0, -bound_exp(2.f * __uint_as_float(*f.src_max)));
     uint8_t *blk = reinterpret_cast<uint8_t *>(f.dst);
     if (!f.by_rows) {
         const int he = (C + 1) / 2, ho = C - he, mid = (C - 1) / 2;
@@ -830,18 +702,18 @@ __global__ void __launch_bounds__(128) k_fold_slices(const __grid_constant__ Fol
             const bool isv = y >= Rp;
             const int r = isv ? y - Rp : y;
             const int KT = isv ? KTv : KTu, groups = KT * TL_K / 4;
-            const float *row = f.src + (int64_t)(r < R ? r : 0) * ldc;
+            const T *row = f.src + (int64_t)(r < R ? r : 0) * ldc;
             for (int t = threadIdx.x; t < groups; t += blockDim.x) {
-                float v[4];
+                T v[4];
 #pragma unroll
                 for (int e = 0; e < 4; e++) {
                     const int j = 4 * t + e;
-                    if (r >= R) v[e] = 0.f;
-                    else if (!isv) v[e] = j < mid ? row[j] + row[C - 1 - j] : (j == mid ? row[mid] : 0.f);
-                    else v[e] = j < ho ? row[j] - row[C - 1 - j] : 0.f;
+                    if (r >= R) v[e] = T(0);
+                    else if (!isv) v[e] = j < mid ? row[j] + row[C - 1 - j] : (j == mid ? row[mid] : T(0));
+                    else v[e] = j < ho ? row[j] - row[C - 1 - j] : T(0);
                 }
-                if (!isv) put_slices4(blk, pu, a_tile_off(r, 4 * t, KTu), v, scale);
-                else put_slices4(blk + 4 * pu, pv, a_tile_off(r, 4 * t, KTv), v, scale);
+                if (!isv) put_slices4<NS>(blk, pu, a_tile_off(r, 4 * t, KTu), v, scale);
+                else put_slices4<NS>(blk + NS * pu, pv, a_tile_off(r, 4 * t, KTv), v, scale);
             }
         }
     } else {
@@ -854,53 +726,19 @@ __global__ void __launch_bounds__(128) k_fold_slices(const __grid_constant__ Fol
             const bool isv = y >= Kpu;
             const int k = isv ? y - Kpu : y;
             const bool valid = isv ? k < ho : k < he;
-            const float *ra = f.src + (int64_t)(valid ? k : 0) * ldc;
-            const float *rb = f.src + (int64_t)(valid ? R - 1 - k : 0) * ldc;
+            const T *ra = f.src + (int64_t)(valid ? k : 0) * ldc;
+            const T *rb = f.src + (int64_t)(valid ? R - 1 - k : 0) * ldc;
             const bool single = !isv && k == mid;
             for (int t = threadIdx.x; t < groups; t += blockDim.x) {
-                float v[4];
+                T v[4];
 #pragma unroll
                 for (int e = 0; e < 4; e++) {
                     const int n = 4 * t + e;
-                    v[e] = (!valid || n >= C) ? 0.f
+                    v[e] = (!valid || n >= C) ? T(0)
                          : (single ? ra[n] : (isv ? ra[n] - rb[n] : ra[n] + rb[n]));
                 }
-                if (!isv) put_slices4(blk, pu, b_tile_off(k, 4 * t, KTu), v, scale);
-                else put_slices4(blk + 4 * pu, pv, b_tile_off(k, 4 * t, KTv), v, scale);
-            }
-        }
-    }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(256) k_fold(const __grid_constant__ FoldBatch<T> fb)
-{
-    // blockIdx.y: row, x: columns (grid-stride), z: problem
-    const FoldDesc<T> &f = fb.d[blockIdx.z];
-    const int R = f.R, C = f.C, ldc = ld2(C);
-    for (int i = blockIdx.y; i < R; i += gridDim.y) {
-        for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < C; j += gridDim.x * blockDim.x) {
-            if (!f.by_rows) {
-                const int he = (C + 1) / 2, mid = (C - 1) / 2;
-                const T *row = f.src + (int64_t)i * ldc;
-                if (j < he) {
-                    f.dst[(int64_t)i * ld2(he) + j] = j < mid ? row[j] + row[C - 1 - j] : row[mid];
-                } else {
-                    const int jj = j - he;
-                    T *V = f.dst + (int64_t)R * ld2(he);
-                    V[(int64_t)i * ld2(C - he) + jj] = row[jj] - row[C - 1 - jj];
-                }
-            } else {
-                const int he = (R + 1) / 2, mid = (R - 1) / 2;
-                T v;
-                if (i < he) {
-                    v = i < mid ? f.src[(int64_t)i * ldc + j] + f.src[(int64_t)(R - 1 - i) * ldc + j]
-                                : f.src[(int64_t)mid * ldc + j];
-                } else {
-                    const int ii = i - he;
-                    v = f.src[(int64_t)ii * ldc + j] - f.src[(int64_t)(R - 1 - ii) * ldc + j];
-                }
-                f.dst[(int64_t)i * ldc + j] = v;
+                if (!isv) put_slices4<NS>(blk, pu, b_tile_off(k, 4 * t, KTu), v, scale);
+                else put_slices4<NS>(blk + NS * pu, pv, b_tile_off(k, 4 * t, KTv), v, scale);
             }
         }
     }
@@ -961,13 +799,13 @@ __device__ __forceinline__ void rhs_node(const RhsArgs &a, const double (*s_ro)[
     const double By_rhs = -(djz_dx - djx_dxi - a.c * a.By[t]);
     if (i >= 1 && i < N - 1) {
         const int64_t o = (int64_t)(i - 1) * ldN + j;
-        X0[o] = (T)Ey_rhs; mx[0] = fmaxf(mx[0], fabsf((float)Ey_rhs));
-        X1[o] = (T)Bx_rhs; mx[1] = fmaxf(mx[1], fabsf((float)Bx_rhs));
+        X0[o] = (T)Ey_rhs; mx[0] = fmaxf(mx[0], abs_bound((T)Ey_rhs));
+        X1[o] = (T)Bx_rhs; mx[1] = fmaxf(mx[1], abs_bound((T)Bx_rhs));
     }
     if (j >= 1 && j < N - 1) {
         const int64_t o = (int64_t)i * ldn + (j - 1);
-        X2[o] = (T)Ex_rhs; mx[2] = fmaxf(mx[2], fabsf((float)Ex_rhs));
-        X3[o] = (T)By_rhs; mx[3] = fmaxf(mx[3], fabsf((float)By_rhs));
+        X2[o] = (T)Ex_rhs; mx[2] = fmaxf(mx[2], abs_bound((T)Ex_rhs));
+        X3[o] = (T)By_rhs; mx[3] = fmaxf(mx[3], abs_bound((T)By_rhs));
     }
     double djx_dy = 0, djy_dx = 0;
     if (inner) {
@@ -976,18 +814,18 @@ __device__ __forceinline__ void rhs_node(const RhsArgs &a, const double (*s_ro)[
     }
     const double bz_rhs = -(djx_dy - djy_dx) / h2;
     X6[(int64_t)i * ldN + j] = (T)bz_rhs;
-    mx[6] = fmaxf(mx[6], fabsf((float)bz_rhs));
+    mx[6] = fmaxf(mx[6], abs_bound((T)bz_rhs));
     if (inner) {
         const int64_t o = (int64_t)(i - 1) * ldn + (j - 1);
         const double djx_dx = s_jx[li + 1][lj] - s_jx[li - 1][lj];
         const double djy_dy = s_jy[li][lj + 1] - s_jy[li][lj - 1];
         const double ez_rhs = -(djx_dx + djy_dy) / h2;
         X4[o] = (T)ez_rhs;
-        mx[4] = fmaxf(mx[4], fabsf((float)ez_rhs));
+        mx[4] = fmaxf(mx[4], abs_bound((T)ez_rhs));
         if (a.with_phi) {
             const double phi_rhs = psum(a.ro_f, a.n_f, plane, t) - psum(a.jz_f, a.n_f, plane, t);
             X5[o] = (T)phi_rhs;
-            mx[5] = fmaxf(mx[5], fabsf((float)phi_rhs));
+            mx[5] = fmaxf(mx[5], abs_bound((T)phi_rhs));
         }
     }
 }
@@ -1094,15 +932,14 @@ struct Work {
     unsigned *amax[2];    // per-problem operand maxima, alternating between folds
 };
 
-// A workspace slot holds one problem's matrix: FP64 or FP32 rows of up to
-// N + 4 elements, or in mixed precision the four tiled int8 slice planes of
-// a folded matrix.
+// A workspace slot holds one problem's matrix: natural rows of up to N + 4
+// elements, or the tiled int8 slice planes of a folded matrix.
 template <typename T>
 static size_t slot_elems(int N)
 {
-    // mixed: four tiled slice planes of both fold halves, at most
-    // (N + 127) x (N + 64) bytes each, i.e. that many FP32 words
-    const size_t e = sizeof(T) == sizeof(float) ? (size_t)(N + 128) * (N + 64) : (size_t)N * (N + 4);
+    // the sizeof(T) tiled slice planes of both fold halves take at most
+    // (N + 127) x (N + 64) bytes each, i.e. that many elements of T
+    const size_t e = (size_t)(N + 128) * (N + 64);
     return (e + 31) / 32 * 32;
 }
 
@@ -1137,66 +974,32 @@ static Work<T> carve(void *ws, int N)
     return w;
 }
 
-template <int WM, int WN, int ST, int EPI>
-static int launch_dmma_cfg(const GemmBatch<double> &b, int nsub, int maxM, int maxN,
-                           cudaStream_t st)
-{
-    using Cfg = DmmaCfg<WM, WN, ST>;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_gemm_dmma<WM, WN, ST, EPI>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)Cfg::smem);
-        if (e != cudaSuccess) return cuda_check(e, "dmma smem attribute");
-        attr = true;
-    }
-    dim3 grid((maxN + Cfg::BN - 1) / Cfg::BN, (maxM + Cfg::BM - 1) / Cfg::BM, nsub);
-    k_gemm_dmma<WM, WN, ST, EPI><<<grid, Cfg::NT, Cfg::smem, st>>>(b);
-    return LCB_OK;
-}
-
-template <int EPI>
-static int launch_dmma(const GemmBatch<double> &b, int nsub, int maxM, int maxN, int N,
-                       cudaStream_t st)
-{
-    if (N > 200) return launch_dmma_cfg<2, 2, 3, EPI>(b, nsub, maxM, maxN, st);
-    return launch_dmma_cfg<1, 1, 3, EPI>(b, nsub, maxM, maxN, st);
-}
-
-template <int EPI>
-static int launch_f32(const GemmBatch<float> &b, int nsub, int maxM, int maxN, int N,
-                      cudaStream_t st)
+template <typename T, int EPI>
+static int launch_i8(const GemmBatch<T> &b, int nsub, int maxM, int maxN, cudaStream_t st)
 {
     constexpr int BN = 64;
-    using Cfg = I8Cfg<BN>;
+    using Cfg = I8Cfg<Slices<T>::n, BN>;
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_gemm_i8<BN, EPI>,
+        cudaError_t e = cudaFuncSetAttribute(k_gemm_i8<T, BN, EPI>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)Cfg::smem);
         if (e != cudaSuccess) return cuda_check(e, "i8 gemm smem attribute");
         attr = true;
     }
-    (void)N;
     dim3 grid((maxN + BN - 1) / BN, (maxM + I8_BM - 1) / I8_BM, nsub);
-    k_gemm_i8<BN, EPI><<<grid, 256, Cfg::smem, st>>>(b);
+    k_gemm_i8<T, BN, EPI><<<grid, 256, Cfg::smem, st>>>(b);
     return LCB_OK;
 }
 
-static int launch_wave(const GemmBatch<double> &b, int nsub, int epi, int maxM, int maxN,
+template <typename T>
+static int launch_wave(const GemmBatch<T> &b, int nsub, int epi, int maxM, int maxN,
                        int N, cudaStream_t st)
 {
-    if (epi == EPI_STORE) return launch_dmma<EPI_STORE>(b, nsub, maxM, maxN, N, st);
-    if (epi == EPI_SCALE) return launch_dmma<EPI_SCALE>(b, nsub, maxM, maxN, N, st);
-    return launch_dmma<EPI_FIELD>(b, nsub, maxM, maxN, N, st);
-}
-
-static int launch_wave(const GemmBatch<float> &b, int nsub, int epi, int maxM, int maxN,
-                       int N, cudaStream_t st)
-{
-    if (epi == EPI_STORE) return launch_f32<EPI_STORE>(b, nsub, maxM, maxN, N, st);
-    if (epi == EPI_SCALE) return launch_f32<EPI_SCALE>(b, nsub, maxM, maxN, N, st);
-    return launch_f32<EPI_FIELD>(b, nsub, maxM, maxN, N, st);
+    (void)N;
+    if (epi == EPI_STORE) return launch_i8<T, EPI_STORE>(b, nsub, maxM, maxN, st);
+    if (epi == EPI_SCALE) return launch_i8<T, EPI_SCALE>(b, nsub, maxM, maxN, st);
+    return launch_i8<T, EPI_FIELD>(b, nsub, maxM, maxN, st);
 }
 
 template <typename T>
@@ -1217,8 +1020,9 @@ static int run_wave(const GemmBatch<T> &b, int nsub, int epi, int N, cudaStream_
 template <typename T>
 static int run_fold(T *const *src, T *const *dst, const int *probs, int np, const int *rows,
                     const int *cols, int by_rows, int N, cudaStream_t st,
-                    const unsigned *src_max = nullptr, unsigned *clear = nullptr)
+                    const unsigned *src_max, unsigned *clear)
 {
+    LCB_REQUIRE(src_max, "fold without operand maxima");
     FoldBatch<T> fb;
     memset(&fb, 0, sizeof(fb));
     for (int q = 0; q < np; q++) {
@@ -1231,21 +1035,12 @@ static int run_fold(T *const *src, T *const *dst, const int *probs, int np, cons
         fb.d[q].src_max = src_max ? src_max + p : nullptr;
     }
     fb.clear = clear;
-    if constexpr (sizeof(T) == sizeof(float)) {
-        if (src_max) {
-            // output rows: 2 x 128-padded rows (column fold) or the two
-            // 32-padded halves (row fold), four per block
-            const int nrows = by_rows ? ntiles((N + 1) / 2, TL_K) * TL_K * 2
-                                      : 2 * ntiles(N, TL_M) * TL_M;
-            dim3 grid(1u, (unsigned)((nrows + 3) / 4), np);
-            k_fold_slices<<<grid, dim3(32, 4), 0, st>>>(fb);
-            LCB_LAUNCH_CHECK("k_fold_slices");
-            return LCB_OK;
-        }
-    }
-    dim3 grid((unsigned)((N + 255) / 256), (unsigned)N, np);
-    k_fold<T><<<grid, 256, 0, st>>>(fb);
-    LCB_LAUNCH_CHECK("k_fold");
+    // output rows: 2 x 128-padded rows (column fold) or the two 32-padded
+    // halves (row fold), four per block
+    const int nrows = by_rows ? ntiles((N + 1) / 2, TL_K) * TL_K * 2 : 2 * ntiles(N, TL_M) * TL_M;
+    dim3 grid(1u, (unsigned)((nrows + 3) / 4), np);
+    k_fold_slices<T><<<grid, dim3(32, 4), 0, st>>>(fb);
+    LCB_LAUNCH_CHECK("k_fold_slices");
     return LCB_OK;
 }
 
@@ -1253,7 +1048,7 @@ template <typename T>
 static int solve(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st)
 {
     const int N = a->grid_steps, n = N - 2;
-    const OpLayout L = op_layout(N, sizeof(T) == sizeof(float));
+    const OpLayout L = op_layout(N);
     Work<T> w = carve<T>(a->workspace, N);
     // Phi (problem 5) is skipped when neither of its outputs is wanted.
     const bool with_phi = a->out_half.f[6] || a->out_full.f[6];
@@ -1276,7 +1071,7 @@ static int solve(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st
     // int8 slices (the right-hand sides, waves 1-3) records its largest
     // element per problem; the maxima alternate between two arrays, each
     // fold clearing the one that the next wave fills
-    constexpr bool rec = sizeof(T) == sizeof(float);
+    constexpr bool rec = true;
     unsigned *const mx0 = rec ? w.amax[0] : nullptr, *const mx1 = rec ? w.amax[1] : nullptr;
     unsigned *cur_mx = nullptr;
     r.amax_out = mx0;
@@ -1327,7 +1122,7 @@ static int solve(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st
                 if (rec) {
                     // tiled slice planes (A role): U block, then V block
                     const uint8_t *base = reinterpret_cast<const uint8_t *>(w.S2[p]);
-                    d.A = reinterpret_cast<const T *>(base + (par ? 4 * a_plane_bytes(rows[p], he) : 0));
+                    d.A = reinterpret_cast<const T *>(base + (par ? Slices<T>::n * a_plane_bytes(rows[p], he) : 0));
                     d.a_plane = (int)a_plane_bytes(rows[p], d.K);
                     d.b_plane = (int)b_plane_bytes((int)L.rows[id], (int)L.cols[id]);
                 }
@@ -1356,7 +1151,7 @@ static int solve(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st
                 if (rec) {
                     // tiled slice planes (B role): U block, then V block
                     const uint8_t *base = reinterpret_cast<const uint8_t *>(w.S2[p]);
-                    d.B = reinterpret_cast<const T *>(base + (par ? 4 * b_plane_bytes(he, cols[p]) : 0));
+                    d.B = reinterpret_cast<const T *>(base + (par ? Slices<T>::n * b_plane_bytes(he, cols[p]) : 0));
                     d.b_plane = (int)b_plane_bytes(d.K, cols[p]);
                     d.a_plane = (int)a_plane_bytes((int)L.rows[id], (int)L.cols[id]);
                 }
@@ -1427,7 +1222,7 @@ extern "C" size_t lcb_field_operators_bytes(int grid_steps, int precision)
 {
     if (grid_steps < 5 || (grid_steps % 2) == 0) return 0;
     const size_t el = precision == LCB_PREC_MIXED ? sizeof(float) : sizeof(double);
-    return (size_t)op_layout(grid_steps, precision == LCB_PREC_MIXED).off[OP_COUNT] * el;
+    return (size_t)op_layout(grid_steps).off[OP_COUNT] * el;
 }
 
 extern "C" int lcb_field_operators_build(int grid_steps, double h, double subtraction_coeff,
@@ -1442,21 +1237,23 @@ extern "C" int lcb_field_operators_build(int grid_steps, double h, double subtra
                 lcb_field_operators_bytes(N, precision));
     LCB_REQUIRE(((uintptr_t)operators & 255) == 0, "operator buffer must be 256-byte aligned");
     LCB_REQUIRE(h > 0, "transverse step must be > 0");
-    const OpLayout L = op_layout(N, precision == LCB_PREC_MIXED);
+    const OpLayout L = op_layout(N);
     const int blocks = (int)((L.off[OP_COUNT] + 255) / 256);
+    const int sblocks = (int)((L.off[OP_D] + 255) / 256);
+    // spectral matrices in the solver's precision, then the transform blocks
+    // as int8 slice planes (four for FP32 operands, eight for FP64)
     if (precision == LCB_PREC_MIXED) {
         k_build_ops<float><<<blocks, 256, 0, as_stream(stream)>>>(
             N, h, subtraction_coeff, L, static_cast<float *>(operators));
         LCB_LAUNCH_CHECK("k_build_ops");
-        // then the transform blocks are overwritten with their slice planes
-        k_build_slices<<<(int)((L.off[OP_D] + 255) / 256), 256, 0, as_stream(stream)>>>(
-            N, L, static_cast<uint8_t *>(operators));
-        LCB_LAUNCH_CHECK("k_build_slices");
-        return LCB_OK;
-    } else
+        k_build_slices<4><<<sblocks, 256, 0, as_stream(stream)>>>(N, L, static_cast<uint8_t *>(operators));
+    } else {
         k_build_ops<double><<<blocks, 256, 0, as_stream(stream)>>>(
             N, h, subtraction_coeff, L, static_cast<double *>(operators));
-    LCB_LAUNCH_CHECK("k_build_ops");
+        LCB_LAUNCH_CHECK("k_build_ops");
+        k_build_slices<8><<<sblocks, 256, 0, as_stream(stream)>>>(N, L, static_cast<uint8_t *>(operators));
+    }
+    LCB_LAUNCH_CHECK("k_build_slices");
     return LCB_OK;
 }
 
@@ -1537,8 +1334,8 @@ extern "C" int lcb_compute_fields_noalloc(const lcb_compute_fields_args *a, void
     LCB_REQUIRE(need > 0, "grid_steps must be odd and >= 5 (got %d)", a->grid_steps);
     LCB_REQUIRE(need <= LCB_NOALLOC_FIELDS_SCRATCH_BYTES,
                 "grid_steps %d in precision %d needs %zu bytes of scratch; the "
-                "allocation-free entry point has %zu (largest grid: 261 in FP64, "
-                "277 in mixed precision) -- use lcb_compute_fields with a workspace",
+                "allocation-free entry point has %zu (largest grid: 283 in FP64, "
+                "427 in mixed precision) -- use lcb_compute_fields with a workspace",
                 a->grid_steps, a->precision, need, (size_t)LCB_NOALLOC_FIELDS_SCRATCH_BYTES);
     void *scratch = nullptr;
     int rc = scratch_address(&scratch);

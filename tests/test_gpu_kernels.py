@@ -351,10 +351,10 @@ def _op_layout(N, mixed=False):
     offs, lds, o = [], [], 0
     for i, (r, c) in enumerate(shapes):
         # transform blocks: even row stride (FP64), or four tiled int8 slice planes
-        ld = c if (mixed or i >= 8) else (c + 1) // 2 * 2
+        ld = c
         offs.append(o)
         lds.append(ld)
-        words = _plane_bytes(i, r, c) if (mixed and i < 8) else r * ld
+        words = _plane_bytes(i, r, c) if i < 8 else r * ld
         o += (words + 31) // 32 * 32
     return shapes, offs, lds
 
@@ -406,15 +406,17 @@ def test_field_operators_build(N, mixed):
     shapes, offs, lds = _op_layout(N, mixed)
     rel = 1e-6 if mixed else 1e-13
     raw = ops.buf.cpu().numpy().view(np.uint8)
+    ns = 4 if mixed else 8          # slices per element = bytes per element
     for i, (ref, shp, off, ld) in enumerate(zip(blocks, shapes, offs, lds)):
-        if mixed and i < 8:
-            # four tiled int8 slice planes, x = 2 sum_k s_k 2^-(6 + 7 k)
+        if i < 8:
+            # ns tiled int8 slice planes, x = 2 sum_k s_k 2^-(6 + 7 k)
             plane = _plane_bytes(i, *shp)
             at = _tile_offsets(i, *shp)
-            planes = [raw[4 * off + k * plane:4 * off + (k + 1) * plane].view(np.int8)[at]
-                      .astype(np.float64) for k in range(4)]
+            planes = [raw[ns * off + k * plane:ns * off + (k + 1) * plane].view(np.int8)[at]
+                      .astype(np.float64) for k in range(ns)]
             got = 2 * sum(p * 2.0 ** -(6 + 7 * k) for k, p in enumerate(planes))
-            rel_b = 2.0 ** -23  # FP32 rounding of the value, then exact slices
+            # FP32 rounding of the value, then exact slices (mixed); FP64
+            rel_b = 2.0 ** -23 if mixed else 1e-15
         else:
             got = buf[off:off + shp[0] * ld].reshape(shp[0], ld)[:, :shp[1]]
             rel_b = rel
