@@ -1,5 +1,7 @@
 // Plasma particle kernels: free-streaming estimate, fused gather + push, and
 // tiled charge/current deposition.  FP64 particles (SoA, coalesced).
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace lcb {
@@ -271,61 +273,105 @@ k_deposit_tiled(int64_t n_per_sort, int Ns, int N, double h,
                 const double *__restrict__ m_a, Acc *ro, Acc *jx, Acc *jy, Acc *jz,
                 int *err)
 {
+    static_assert(DEP_PPT == 2, "a thread owns two particles");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Acc *sw = reinterpret_cast<Acc *>(smem_raw);  // [4][WX][WY]
     constexpr int WSZ = DEP_WX * DEP_WY;
     const int s = blockIdx.z;
-    const int i0 = blockIdx.y * DEP_TI, j0 = blockIdx.x * DEP_TJ;
     const int64_t base = (int64_t)s * n_per_sort;
     const int half_n = N / 2;
     const int64_t NN = (int64_t)N * N;
     Acc *gro = ro + s * NN, *gjx = jx + s * NN, *gjy = jy + s * NN, *gjz = jz + s * NN;
 
     for (int t = threadIdx.x; t < 4 * WSZ; t += blockDim.x) sw[t] = Acc(0);
-    // window origin from the tile's first particle's initial lattice position
+    // Tiles start on a lattice row whose cell also holds the next row, so
+    // that a thread's two particles (slots t and t + DEP_THREADS: lattice
+    // rows ti and ti + 1, ti even) usually share a cell; the grid has one
+    // spare row of tiles for the shift.
     double dummy;
-    const int64_t k0 = base + (int64_t)i0 * Ns + j0;
+    int off = 0;
+    if (Ns > 1 && cell_of(x_init[base] / h + 0.5, half_n, dummy) !=
+                  cell_of(x_init[base + Ns] / h + 0.5, half_n, dummy))
+        off = 1;
+    const int i0 = blockIdx.y * DEP_TI - off, j0 = blockIdx.x * DEP_TJ;
+    const int ir = i0 < 0 ? 0 : i0;
+    if (ir >= Ns) return;
+    // window origin from the tile's first particle's initial lattice position
+    const int64_t k0 = base + (int64_t)ir * Ns + j0;
     const int wx0 = cell_of(x_init[k0] / h + 0.5, half_n, dummy) - 2 - DEP_SLACK;
     const int wy0 = cell_of(y_init[k0] / h + 0.5, half_n, dummy) - 2 - DEP_SLACK;
     // lattice spacing along x: two particles per cell?
     bool two = false;
-    if (i0 + 1 < Ns) {
+    if (ir + 1 < Ns) {
         const double d = x_init[k0 + Ns] - x_init[k0];
         two = fabs(2 * d - h) < 0.25 * h;
     }
     __syncthreads();
 
+    bool dep[2];
+    double v[2][4], xl[2], yl[2];
+    int ix[2], iy[2];
 #pragma unroll
     for (int r = 0; r < DEP_PPT; r++) {
         int ti, tj;
         tile_slot(threadIdx.x + r * DEP_THREADS, two, ti, tj);
         const int i = i0 + ti, j = j0 + tj;
-        bool dep = i < Ns && j < Ns;
-        double dro = 0, djx = 0, djy = 0, djz = 0, xl = 0, yl = 0;
-        int ix = 0, iy = 0;
-        if (dep) {
+        dep[r] = i >= 0 && i < Ns && j < Ns;
+        v[r][0] = v[r][1] = v[r][2] = v[r][3] = 0;
+        xl[r] = yl[r] = 0;
+        ix[r] = iy[r] = -1000;
+        if (dep[r]) {
             const int64_t k = base + (int64_t)i * Ns + j;
             const double q = q_a[k];
             if (q == 0) {
-                dep = false;
+                dep[r] = false;
             } else {
                 const double m = m_a[k], px = px_a[k], py = py_a[k], pz = pz_a[k];
                 const double gm = sqrt(m * m + px * px + py * py + pz * pz);
                 const double ig = 1.0 / gm;
-                dro = q / (1 - pz * ig);
+                const double dro = q / (1 - pz * ig);
                 const double rg = dro * ig;
-                djx = px * rg; djy = py * rg; djz = pz * rg;
-                check_range<Acc>(dro, djx, djy, djz, 1.0 / h, err);
-                ix = cell_of((x_init[k] + x_offt[k]) / h + 0.5, half_n, xl);
-                iy = cell_of((y_init[k] + y_offt[k]) / h + 0.5, half_n, yl);
-                if (!(ix >= 2 && ix < N - 2 && iy >= 2 && iy < N - 2)) {
+                v[r][0] = dro; v[r][1] = px * rg; v[r][2] = py * rg; v[r][3] = pz * rg;
+                check_range<Acc>(v[r][0], v[r][1], v[r][2], v[r][3], 1.0 / h, err);
+                ix[r] = cell_of((x_init[k] + x_offt[k]) / h + 0.5, half_n, xl[r]);
+                iy[r] = cell_of((y_init[k] + y_offt[k]) / h + 0.5, half_n, yl[r]);
+                if (!(ix[r] >= 2 && ix[r] < N - 2 && iy[r] >= 2 && iy[r] < N - 2)) {
                     if (err) atomicOr(err, LCB_DEVERR_PLASMA_STENCIL);
-                    dep = false;
+                    dep[r] = false;
                 }
             }
         }
-        deposit_one<Acc, DEP_WX, DEP_WY>(sw, gro, gjx, gjy, gjz, N, h, wx0, wy0, dep, ix, iy,
-                                          xl, yl, dro, djx, djy, djz);
+    }
+    // FP64: two particles in one cell add their contributions before the
+    // shared atomic (one atomic per stencil point and quantity for both)
+    const int lx = ix[0] - 2 - wx0, ly = iy[0] - 2 - wy0;
+    const bool joint = sizeof(Acc) == sizeof(double) && !std::is_integral<Acc>::value &&
+                       dep[0] && dep[1] && ix[0] == ix[1] && iy[0] == iy[1] &&
+                       lx >= 0 && lx + 5 <= DEP_WX && ly >= 0 && ly + 5 <= DEP_WY;
+    if (joint) {
+        double ax[5], ay[5], bx[5], by[5];
+        weights4(xl[0], ax); weights4(yl[0], ay);
+        weights4(xl[1], bx); weights4(yl[1], by);
+        const double ih = 1.0 / h;
+#pragma unroll
+        for (int b = 0; b < 5; b++) { ay[b] *= ih; by[b] *= ih; }
+#pragma unroll
+        for (int a = 0; a < 5; a++) {
+            const double xa = ax[a] * ih, xb = bx[a] * ih;
+#pragma unroll
+            for (int b = 0; b < 5; b++) {
+                const double wa = xa * ay[b], wb = xb * by[b];
+                const int c = (lx + a) * DEP_WY + ly + b;
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    atomicAdd(sw + q * WSZ + c, Acc(fma(v[0][q], wa, v[1][q] * wb)));
+            }
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r < DEP_PPT; r++)
+            deposit_one<Acc, DEP_WX, DEP_WY>(sw, gro, gjx, gjy, gjz, N, h, wx0, wy0, dep[r], ix[r],
+                                              iy[r], xl[r], yl[r], v[r][0], v[r][1], v[r][2], v[r][3]);
     }
     __syncthreads();
     for (int t = threadIdx.x; t < WSZ; t += blockDim.x) {
@@ -1073,7 +1119,7 @@ static int deposit_fixed(int64_t n_per_sort, int n_sorts, int N, double h, int p
     if (e != cudaSuccess) return cuda_check(e, "memset fixed-point sums");
     if (n_per_sort > 0) {
         const dim3 grid((particles_side + DEP_TJ - 1) / DEP_TJ,
-                        (particles_side + DEP_TI - 1) / DEP_TI, n_sorts);
+                        (particles_side + 1 + DEP_TI - 1) / DEP_TI, n_sorts);   // spare tile row
         const size_t sm = deposit_smem_bytes<fix_t>();
         static bool attr = false;
         if (!attr) {
@@ -1167,7 +1213,7 @@ extern "C" int lcb_plasma_deposit(
     }
     if (n_per_sort > 0) {
         dim3 grid((particles_side + DEP_TJ - 1) / DEP_TJ,
-                  (particles_side + DEP_TI - 1) / DEP_TI, n_sorts);
+                  (particles_side + 1 + DEP_TI - 1) / DEP_TI, n_sorts);   // spare tile row
         {
             const size_t sm = deposit_smem_bytes<double>();
             static bool attr = false;
