@@ -395,260 +395,19 @@ static size_t deposit_smem_bytes()
 // ---------------------------------------------------------------------------
 // Fused predictor-corrector stage: K2 (move_smart) followed by K3 (deposit)
 // of the same particles, and for the first stage of an xi step K1 (the
-// free-streaming estimate) in front.  A block owns a lattice tile of TI x TJ
-// particles; the six field planes are staged in a shared-memory window around
-// the tile for the midpoint gather, the new position is deposited into a
-// second window, flushed with global atomics.  Particles whose stencil leaves
-// a window use global memory directly, so the result never depends on the
-// tiling.  Each particle's arithmetic is exactly that of K1, K2 and K3.
-// ---------------------------------------------------------------------------
-template <int WX, int WY>
-struct MdWin {
-    static constexpr int WSZ = WX * WY;
-};
-
-template <typename Acc, int WX, int WY, bool FIRST>
-__global__ void __launch_bounds__(DEP_THREADS)
-k_move_deposit(int64_t n_per_sort, int Ns, int N, double h, double xi_step, double boundary,
-               const double *__restrict__ Exf, const double *__restrict__ Eyf,
-               const double *__restrict__ Ezf, const double *__restrict__ Bxf,
-               const double *__restrict__ Byf, const double *__restrict__ Bzf,
-               const double *__restrict__ x_init, const double *__restrict__ y_init,
-               const double *__restrict__ xo_p, const double *__restrict__ yo_p,
-               const double *__restrict__ px_p, const double *__restrict__ py_p,
-               const double *__restrict__ pz_p, const double *__restrict__ q_p,
-               const double *__restrict__ m_a,
-               double *q_f, double *xo_f, double *yo_f, double *px_f, double *py_f,
-               double *pz_f, Acc *ro, Acc *jx, Acc *jy, Acc *jz, int *err)
-{
-    constexpr int WSZ = WX * WY;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *sf = reinterpret_cast<double *>(smem_raw);          // [6][WX][WY] fields
-    Acc *sw = reinterpret_cast<Acc *>(sf + 6 * WSZ);           // [4][WX][WY] deposit
-    const int s = blockIdx.z;
-    const int i0 = blockIdx.y * DEP_TI, j0 = blockIdx.x * DEP_TJ;
-    const int64_t base = (int64_t)s * n_per_sort;
-    const int half_n = N / 2;
-    const int64_t NN = (int64_t)N * N;
-    Acc *gro = ro + s * NN, *gjx = jx + s * NN, *gjy = jy + s * NN, *gjz = jz + s * NN;
-    const double *fld[6] = {Exf, Eyf, Ezf, Bxf, Byf, Bzf};
-
-    double dummy;
-    const int64_t k0 = base + (int64_t)i0 * Ns + j0;
-    const int wx0 = cell_of(x_init[k0] / h + 0.5, half_n, dummy) - 2 - DEP_SLACK;
-    const int wy0 = cell_of(y_init[k0] / h + 0.5, half_n, dummy) - 2 - DEP_SLACK;
-    bool two = false;
-    if (i0 + 1 < Ns) {
-        const double d = x_init[k0 + Ns] - x_init[k0];
-        two = fabs(2 * d - h) < 0.25 * h;
-    }
-    for (int t = threadIdx.x; t < 4 * WSZ; t += blockDim.x) sw[t] = Acc(0);
-    for (int t = threadIdx.x; t < WSZ; t += blockDim.x) {
-        const int gx = wx0 + t / WY, gy = wy0 + t % WY;
-        const bool in = gx >= 0 && gx < N && gy >= 0 && gy < N;
-        const int64_t g = (int64_t)gx * N + gy;
-#pragma unroll
-        for (int f = 0; f < 6; f++) sf[f * WSZ + t] = in ? __ldg(fld[f] + g) : 0.0;
-    }
-    __syncthreads();
-
-#pragma unroll
-    for (int r = 0; r < DEP_PPT; r++) {
-        int ti, tj;
-        tile_slot(threadIdx.x + r * DEP_THREADS, two, ti, tj);
-        const int i = i0 + ti, j = j0 + tj;
-        bool dep = false;
-        double dro = 0, djx = 0, djy = 0, djz = 0, xl2 = 0, yl2 = 0;
-        int jx2 = 0, jy2 = 0;
-        if (i < Ns && j < Ns) {
-            const int64_t k = base + (int64_t)i * Ns + j;
-            const double mk = m_a[k];
-            const double opx = px_p[k], opy = py_p[k], opz = pz_p[k];
-            const double xo0 = xo_p[k], yo0 = yo_p[k];
-            double qk, xof, yof;
-            if (FIRST) {
-                // K1: full = prev, offsets free-streamed (move.py:292-313)
-                qk = q_p[k];
-                xof = xo0; yof = yo0;
-                if (mk != 0) {
-                    const double gm = sqrt(mk * mk + opz * opz + opx * opx + opy * opy);
-                    const double adv = xi_step / (gm - opz);
-                    xof += opx * adv;
-                    yof += opy * adv;
-                }
-            } else {
-                qk = q_f[k];
-                xof = xo_f[k]; yof = yo_f[k];
-            }
-            if (qk == 0) {
-                // skipped by K2 (and K3): the full state stays as it is
-                if (FIRST) {
-                    xo_f[k] = xof; yo_f[k] = yof;
-                    px_f[k] = opx; py_f[k] = opy; pz_f[k] = opz;
-                    q_f[k] = qk;
-                }
-            } else {
-                // ---- K2 (move.py:169-289) ----
-                const double xi0 = x_init[k], yi0 = y_init[k];
-                double px = opx, py = opy, pz = opz;
-                double xh = xi0 + (xo0 + xof) / 2;
-                double yh = yi0 + (yo0 + yof) / 2;
-                if (xh > boundary)  { xh =  2 * boundary - xh; px = py = pz = 0; }
-                if (xh < -boundary) { xh = -2 * boundary - xh; px = py = pz = 0; }
-                if (yh > boundary)  { yh =  2 * boundary - yh; px = py = pz = 0; }
-                if (yh < -boundary) { yh = -2 * boundary - yh; px = py = pz = 0; }
-                double xl, yl;
-                const int ix = cell_of(xh / h + 0.5, half_n, xl);
-                const int iy = cell_of(yh / h + 0.5, half_n, yl);
-                double Ex = 0, Ey = 0, Ez = 0, Bx = 0, By = 0, Bz = 0;
-                if (ix >= 2 && ix < N - 2 && iy >= 2 && iy < N - 2) {
-                    double wx[5], wy[5];
-                    weights4(xl, wx);
-                    weights4(yl, wy);
-                    const int lx = ix - 2 - wx0, ly = iy - 2 - wy0;
-                    if (lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY) {
-#pragma unroll
-                        for (int a = 0; a < 5; a++) {
-                            const int row = (lx + a) * WY + ly;
-#pragma unroll
-                            for (int b = 0; b < 5; b++) {
-                                const double w = wx[a] * wy[b];
-                                const int c = row + b;
-                                Ex += sf[c] * w; Bx += sf[3 * WSZ + c] * w;
-                                Ey += sf[WSZ + c] * w; By += sf[4 * WSZ + c] * w;
-                                Ez += sf[2 * WSZ + c] * w; Bz += sf[5 * WSZ + c] * w;
-                            }
-                        }
-                    } else {
-#pragma unroll
-                        for (int a = 0; a < 5; a++) {
-                            const int row = (ix + a - 2) * N + iy - 2;
-#pragma unroll
-                            for (int b = 0; b < 5; b++) {
-                                const double w = wx[a] * wy[b];
-                                const int idx = row + b;
-                                Ex += __ldg(Exf + idx) * w; Bx += __ldg(Bxf + idx) * w;
-                                Ey += __ldg(Eyf + idx) * w; By += __ldg(Byf + idx) * w;
-                                Ez += __ldg(Ezf + idx) * w; Bz += __ldg(Bzf + idx) * w;
-                            }
-                        }
-                    }
-                } else if (err) {
-                    atomicOr(err, LCB_DEVERR_PLASMA_STENCIL);
-                }
-                double gm = sqrt(mk * mk + px * px + py * py + pz * pz);
-                double ig = 1.0 / gm;
-                double vx = px * ig, vy = py * ig, vz = pz * ig;
-                double f = qk * xi_step / (1 - vz);
-                double dpx = f * (Ex + vy * Bz - vz * By);
-                double dpy = f * (Ey - vx * Bz + vz * Bx);
-                double dpz = f * (Ez + vx * By - vy * Bx);
-                px = opx + dpx * 0.5; py = opy + dpy * 0.5; pz = opz + dpz * 0.5;
-                gm = sqrt(mk * mk + px * px + py * py + pz * pz);
-                ig = 1.0 / gm;
-                vx = px * ig; vy = py * ig; vz = pz * ig;
-                f = qk * xi_step / (1 - vz);
-                dpx = f * (Ex + vy * Bz - vz * By);
-                dpy = f * (Ey - vx * Bz + vz * Bx);
-                dpz = f * (Ez + vx * By - vy * Bx);
-                px = opx + dpx * 0.5; py = opy + dpy * 0.5; pz = opz + dpz * 0.5;
-                gm = sqrt(mk * mk + px * px + py * py + pz * pz);
-                const double adv = xi_step / (gm - pz);
-                double xo = xo0 + px * adv;
-                double yo = yo0 + py * adv;
-                px = opx + dpx; py = opy + dpy; pz = opz + dpz;
-                double x = xi0 + xo, y = yi0 + yo;
-                if (x > boundary)  { x =  2 * boundary - x; xo = x - xi0; px = py = pz = 0; }
-                if (x < -boundary) { x = -2 * boundary - x; xo = x - xi0; px = py = pz = 0; }
-                if (y > boundary)  { y =  2 * boundary - y; yo = y - yi0; px = py = pz = 0; }
-                if (y < -boundary) { y = -2 * boundary - y; yo = y - yi0; px = py = pz = 0; }
-                bool absorbed = false;
-                if (x >= boundary || x <= -boundary || y >= boundary || y <= -boundary) {
-                    xo = yo = 0; px = py = pz = 0;
-                    absorbed = true;
-                }
-                xo_f[k] = xo; yo_f[k] = yo;
-                px_f[k] = px; py_f[k] = py; pz_f[k] = pz;
-                if (FIRST || absorbed) q_f[k] = absorbed ? 0.0 : qk;
-                if (!absorbed) {
-                    // ---- K3 on the new state (weights.py:151-190) ----
-                    const double gd = sqrt(mk * mk + px * px + py * py + pz * pz);
-                    const double igd = 1.0 / gd;
-                    dro = qk / (1 - pz * igd);
-                    const double rg = dro * igd;
-                    djx = px * rg; djy = py * rg; djz = pz * rg;
-                    check_range<Acc>(dro, djx, djy, djz, 1.0 / h, err);
-                    jx2 = cell_of((xi0 + xo) / h + 0.5, half_n, xl2);
-                    jy2 = cell_of((yi0 + yo) / h + 0.5, half_n, yl2);
-                    if (jx2 >= 2 && jx2 < N - 2 && jy2 >= 2 && jy2 < N - 2) dep = true;
-                    else if (err) atomicOr(err, LCB_DEVERR_PLASMA_STENCIL);
-                }
-            }
-        }
-        deposit_one<Acc, WX, WY>(sw, gro, gjx, gjy, gjz, N, h, wx0, wy0, dep, jx2, jy2,
-                                  xl2, yl2, dro, djx, djy, djz);
-    }
-    __syncthreads();
-    for (int t = threadIdx.x; t < WSZ; t += blockDim.x) {
-        const int gx = wx0 + t / WY, gy = wy0 + t % WY;
-        if (gx < 0 || gx >= N || gy < 0 || gy >= N) continue;
-        const int64_t c = (int64_t)gx * N + gy;
-        const Acc v0 = sw[t], v1 = sw[WSZ + t], v2 = sw[2 * WSZ + t], v3 = sw[3 * WSZ + t];
-        if (v0 != Acc(0)) atomicAdd(gro + c, v0);
-        if (v1 != Acc(0)) atomicAdd(gjx + c, v1);
-        if (v2 != Acc(0)) atomicAdd(gjy + c, v2);
-        if (v3 != Acc(0)) atomicAdd(gjz + c, v3);
-    }
-}
-
-template <typename Acc, int WX, int WY>
-static size_t move_deposit_smem() { return (size_t)WX * WY * (6 * sizeof(double) + 4 * sizeof(Acc)); }
-
-template <typename Acc, int WX, int WY, bool FIRST>
-static int launch_move_deposit(const lcb_move_deposit_args *a, dim3 grid, Acc *ro, Acc *jx,
-                               Acc *jy, Acc *jz, cudaStream_t st)
-{
-    const size_t sm = move_deposit_smem<Acc, WX, WY>();
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_move_deposit<Acc, WX, WY, FIRST>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (e != cudaSuccess) return cuda_check(e, "move_deposit smem attribute");
-        attr = true;
-    }
-    const lcb_plasma_particles &p = a->prev, &f = a->full;
-    k_move_deposit<Acc, WX, WY, FIRST><<<grid, DEP_THREADS, sm, st>>>(
-        a->n_per_sort, a->particles_side, a->grid_steps, a->h, a->xi_step, a->boundary,
-        a->fields[0], a->fields[1], a->fields[2], a->fields[3], a->fields[4], a->fields[5],
-        p.x_init, p.y_init, p.x_offt, p.y_offt, p.px, p.py, p.pz, p.q, p.m,
-        f.q, f.x_offt, f.y_offt, f.px, f.py, f.pz, ro, jx, jy, jz, a->err);
-    return LCB_OK;
-}
-
-template <typename Acc>
-static int dispatch_move_deposit(const lcb_move_deposit_args *a, dim3 grid, Acc *ro, Acc *jx,
-                                 Acc *jy, Acc *jz, cudaStream_t st)
-{
-    // window: the tile's cells (8 x 16 with two or more particles per cell,
-    // 16 x 32 with one) + 2 stencil + 4 slack on each side
-    const bool small = a->lattice_fineness >= 2;
-    if (small)
-        return a->first ? launch_move_deposit<Acc, 20, 28, true>(a, grid, ro, jx, jy, jz, st)
-                        : launch_move_deposit<Acc, 20, 28, false>(a, grid, ro, jx, jy, jz, st);
-    return a->first ? launch_move_deposit<Acc, DEP_WX, DEP_WY, true>(a, grid, ro, jx, jy, jz, st)
-                    : launch_move_deposit<Acc, DEP_WX, DEP_WY, false>(a, grid, ro, jx, jy, jz, st);
-}
-
-// ---------------------------------------------------------------------------
-// Mixed-precision fused stage: the per-particle algorithm of k_move_deposit
-// with the arithmetic chosen by what each part feeds.  Coordinates and
-// momenta (the push, reflection and absorption) stay FP64.  The midpoint
-// gather reads an FP32 copy of the six field planes' window with FP32
-// weights: the planes themselves come from the FP32 field solve.  The
-// deposit keeps FP64 weights, scales each particle's four values by
-// 2^32 / h^2 once, and rounds every contribution to a 64-bit integer with
-// one FMA against FIX_MAGIC (no conversion instruction), summed with integer
-// atomics.  Sized for three blocks of 256 threads per SM.
+// free-streaming estimate) in front (move.py:169-313, weights.py:151-190).
+// A block owns a lattice tile of TI x TJ particles; the six field planes are
+// staged in a shared-memory window around the tile for the midpoint gather,
+// and the new position is deposited into a second window, flushed with
+// global atomics; particles whose stencil leaves a window use global memory.
+// FP64 (FT = double): each particle's gather and push are those of K2 and
+// K3 (same quotients, same summation order); the deposit sums the two
+// particles of a cell before the shared atomic.  Mixed precision
+// (FT = float): coordinates and momenta stay FP64; the gather reads an FP32
+// copy of the field window with FP32 weights (the planes come from the FP32
+// field solve); the deposit keeps FP64 weights, scales each particle's four
+// values by 2^32 / h^2 once, and rounds every contribution to a 64-bit
+// integer with one FMA against FIX_MAGIC, summed with integer atomics.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void weights4f(float x, float w[5])
 {
@@ -662,30 +421,35 @@ __device__ __forceinline__ void weights4f(float x, float w[5])
     w[4] = b * b * b * b * r24;
 }
 
-// Row stride (in floats) of the FP32 field window: the two half-warps of a
-// warp work one cell apart along x, and a stride of 16 (mod 32) words puts
-// their loads on disjoint banks.
-template <int WY>
-struct FieldStride { static constexpr int v = ((WY + 15) / 32) * 32 + 16; };
+__device__ __forceinline__ void weights_of(float x, float w[5]) { weights4f(x, w); }
+__device__ __forceinline__ void weights_of(double x, double w[5]) { weights4(x, w); }
 
-// Midpoint gather of one particle: FP32 weights, FP32 sums, from the window
-// when the stencil fits in it, else from the FP64 planes in HBM.
-template <int WX, int WY>
-__device__ __forceinline__ void gather_one(const float *sf, const double *const *fld, int N,
-                                           int wx0, int wy0, int ix, int iy, float xl, float yl,
-                                           float F[6])
+// Row stride (in elements) of the field window: the two half-warps of a warp
+// work one cell apart along x, and a row stride of 16 (mod 32) words puts
+// their loads on disjoint banks (FP32: 16 mod 32 elements; FP64: 8 mod 16).
+template <int WY, typename FT>
+struct FieldStride {
+    static constexpr int v = sizeof(FT) == 4 ? ((WY + 15) / 32) * 32 + 16 : ((WY + 7) / 16) * 16 + 8;
+};
+
+// Midpoint gather of one particle from the window when the stencil fits in
+// it, else from the FP64 planes in HBM; weights and sums in FT.
+template <typename FT, int WX, int WY>
+__device__ __forceinline__ void gather_one(const FT *sf, const double *const *fld, int N,
+                                           int wx0, int wy0, int ix, int iy, FT xl, FT yl,
+                                           FT F[6])
 {
-    constexpr int FS = FieldStride<WY>::v, FSZ = WX * FS;
-    float wx[5], wy[5];
-    weights4f(xl, wx);
-    weights4f(yl, wy);
+    constexpr int FS = FieldStride<WY, FT>::v, FSZ = WX * FS;
+    FT wx[5], wy[5];
+    weights_of(xl, wx);
+    weights_of(yl, wy);
     const int lx = ix - 2 - wx0, ly = iy - 2 - wy0;
     if (lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY) {
 #pragma unroll
         for (int a = 0; a < 5; a++) {
 #pragma unroll
             for (int b = 0; b < 5; b++) {
-                const float w = wx[a] * wy[b];
+                const FT w = wx[a] * wy[b];
                 const int c = (lx + a) * FS + ly + b;
 #pragma unroll
                 for (int f = 0; f < 6; f++) F[f] += sf[f * FSZ + c] * w;
@@ -697,9 +461,9 @@ __device__ __forceinline__ void gather_one(const float *sf, const double *const 
             const int row = (ix + a - 2) * N + iy - 2;
 #pragma unroll
             for (int b = 0; b < 5; b++) {
-                const float w = wx[a] * wy[b];
+                const FT w = wx[a] * wy[b];
 #pragma unroll
-                for (int f = 0; f < 6; f++) F[f] += (float)__ldg(fld[f] + row + b) * w;
+                for (int f = 0; f < 6; f++) F[f] += (FT)__ldg(fld[f] + row + b) * w;
             }
         }
     }
@@ -771,9 +535,13 @@ __device__ __forceinline__ void deposit_fix_one(unsigned *swl, int *swh, fix_t *
 // for the two, and their deposits are added before the shared atomics (each
 // contribution is still rounded on its own: fma(sA, wA, fma(sB, wB, M)) adds
 // two integers), which halves the shared-memory traffic of both phases.
-template <int WX, int WY, bool FIRST>
-__global__ void __launch_bounds__(DEP_THREADS, 3)
-k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, double boundary,
+template <typename FT> struct StageAcc;
+template <> struct StageAcc<float> { typedef fix_t type; };
+template <> struct StageAcc<double> { typedef double type; };
+
+template <typename FT, int WX, int WY, bool FIRST>
+__global__ void __launch_bounds__(DEP_THREADS, sizeof(FT) == 4 ? 3 : 2)
+k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step, double boundary,
                   const double *__restrict__ Exf, const double *__restrict__ Eyf,
                   const double *__restrict__ Ezf, const double *__restrict__ Bxf,
                   const double *__restrict__ Byf, const double *__restrict__ Bzf,
@@ -783,21 +551,24 @@ k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, d
                   const double *__restrict__ pz_p, const double *__restrict__ q_p,
                   const double *__restrict__ m_a,
                   double *q_f, double *xo_f, double *yo_f, double *px_f, double *py_f,
-                  double *pz_f, fix_t *ro, fix_t *jx, fix_t *jy, fix_t *jz, int *err)
+                  double *pz_f, typename StageAcc<FT>::type *ro, typename StageAcc<FT>::type *jx,
+                  typename StageAcc<FT>::type *jy, typename StageAcc<FT>::type *jz, int *err)
 {
+    constexpr bool MIXED = sizeof(FT) == 4;
+    typedef typename StageAcc<FT>::type Acc;
     static_assert(DEP_PPT == 2, "a thread owns two particles");
     constexpr int WSZ = WX * WY;
-    constexpr int FS = FieldStride<WY>::v, FSZ = WX * FS;
+    constexpr int FS = FieldStride<WY, FT>::v, FSZ = WX * FS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    fix_t *sw = reinterpret_cast<fix_t *>(smem_raw);           // [4][WX][WY] deposit
-    unsigned *swl = reinterpret_cast<unsigned *>(sw);          //   as [4][WX][WY] low words
+    Acc *sw = reinterpret_cast<Acc *>(smem_raw);               // [4][WX][WY] deposit
+    unsigned *swl = reinterpret_cast<unsigned *>(sw);          //   mixed: [4][WX][WY] low words
     int *swh = reinterpret_cast<int *>(swl + 4 * WSZ);         //   and [4][WX][WY] high words
-    float *sf = reinterpret_cast<float *>(sw + 4 * WSZ);       // [6][WX][FS] fields
+    FT *sf = reinterpret_cast<FT *>(sw + 4 * WSZ);             // [6][WX][FS] fields
     const int s = blockIdx.z;
     const int64_t base = (int64_t)s * n_per_sort;
     const int half_n = N / 2;
     const int64_t NN = (int64_t)N * N;
-    fix_t *const g4[4] = {ro + s * NN, jx + s * NN, jy + s * NN, jz + s * NN};
+    Acc *const g4[4] = {ro + s * NN, jx + s * NN, jy + s * NN, jz + s * NN};
     const double *const fld[6] = {Exf, Eyf, Ezf, Bxf, Byf, Bzf};
     const double ih = 1.0 / h;
 
@@ -821,14 +592,14 @@ k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, d
         const double d = x_init[k0 + Ns] - x_init[k0];
         two = fabs(2 * d - h) < 0.25 * h;
     }
-    for (int t = threadIdx.x; t < 4 * WSZ; t += blockDim.x) sw[t] = 0;
+    for (int t = threadIdx.x; t < 4 * WSZ; t += blockDim.x) sw[t] = Acc(0);
     for (int t = threadIdx.x; t < WSZ; t += blockDim.x) {
         const int gx = wx0 + t / WY, gy = wy0 + t % WY;
         const bool in = gx >= 0 && gx < N && gy >= 0 && gy < N;
         const int64_t g = (int64_t)gx * N + gy;
         const int c = (t / WY) * FS + t % WY;
 #pragma unroll
-        for (int f = 0; f < 6; f++) sf[f * FSZ + c] = in ? (float)__ldg(fld[f] + g) : 0.f;
+        for (int f = 0; f < 6; f++) sf[f * FSZ + c] = in ? (FT)__ldg(fld[f] + g) : FT(0);
     }
     __syncthreads();
 
@@ -836,7 +607,7 @@ k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, d
     int64_t kk[2];
     bool live[2], zero_p[2];
     int ix[2], iy[2];
-    float xlf[2], ylf[2];
+    FT xlf[2], ylf[2];
 #pragma unroll
     for (int p = 0; p < 2; p++) {
         int ti, tj;
@@ -845,7 +616,7 @@ k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, d
         live[p] = i >= 0 && i < Ns && j < Ns;
         zero_p[p] = false;
         ix[p] = iy[p] = -1000;
-        xlf[p] = ylf[p] = 0.f;
+        xlf[p] = ylf[p] = FT(0);
         kk[p] = base + (int64_t)i * Ns + j;
         if (!live[p]) continue;
         const int64_t k = kk[p];
@@ -880,9 +651,10 @@ k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, d
         if (yh < -boundary) { yh = -2 * boundary - yh; z = true; }
         zero_p[p] = z;
         double xl, yl;
-        ix[p] = cell_of(xh * ih + 0.5, half_n, xl);
-        iy[p] = cell_of(yh * ih + 0.5, half_n, yl);
-        xlf[p] = (float)xl; ylf[p] = (float)yl;
+        // FP64: the quotient of K2 itself; mixed: the reciprocal
+        ix[p] = cell_of((MIXED ? xh * ih : xh / h) + 0.5, half_n, xl);
+        iy[p] = cell_of((MIXED ? yh * ih : yh / h) + 0.5, half_n, yl);
+        xlf[p] = (FT)xl; ylf[p] = (FT)yl;
         if (!(ix[p] >= 2 && ix[p] < N - 2 && iy[p] >= 2 && iy[p] < N - 2)) {
             if (err) atomicOr(err, LCB_DEVERR_PLASMA_STENCIL);
             ix[p] = -1000;  // no gather: zero fields, as in the reference's skip
@@ -890,24 +662,24 @@ k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, d
     }
 
     // ---- phase 2: gather ----
-    float F0[6] = {0, 0, 0, 0, 0, 0}, F1[6] = {0, 0, 0, 0, 0, 0};
+    FT F0[6] = {0, 0, 0, 0, 0, 0}, F1[6] = {0, 0, 0, 0, 0, 0};
     {
         const int lx = ix[0] - 2 - wx0, ly = iy[0] - 2 - wy0;
         const bool joint = ix[0] >= 0 && ix[0] == ix[1] && iy[0] == iy[1] &&
                            lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY;
         if (joint) {
-            float ax[5], ay[5], bx[5], by[5];
-            weights4f(xlf[0], ax); weights4f(ylf[0], ay);
-            weights4f(xlf[1], bx); weights4f(ylf[1], by);
+            FT ax[5], ay[5], bx[5], by[5];
+            weights_of(xlf[0], ax); weights_of(ylf[0], ay);
+            weights_of(xlf[1], bx); weights_of(ylf[1], by);
 #pragma unroll
             for (int a = 0; a < 5; a++) {
 #pragma unroll
                 for (int b = 0; b < 5; b++) {
-                    const float wa = ax[a] * ay[b], wb = bx[a] * by[b];
+                    const FT wa = ax[a] * ay[b], wb = bx[a] * by[b];
                     const int c = (lx + a) * FS + ly + b;
 #pragma unroll
                     for (int f = 0; f < 6; f++) {
-                        const float v = sf[f * FSZ + c];
+                        const FT v = sf[f * FSZ + c];
                         F0[f] += v * wa;
                         F1[f] += v * wb;
                     }
@@ -915,9 +687,9 @@ k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, d
             }
         } else {
             if (ix[0] >= 0)
-                gather_one<WX, WY>(sf, fld, N, wx0, wy0, ix[0], iy[0], xlf[0], ylf[0], F0);
+                gather_one<FT, WX, WY>(sf, fld, N, wx0, wy0, ix[0], iy[0], xlf[0], ylf[0], F0);
             if (ix[1] >= 0)
-                gather_one<WX, WY>(sf, fld, N, wx0, wy0, ix[1], iy[1], xlf[1], ylf[1], F1);
+                gather_one<FT, WX, WY>(sf, fld, N, wx0, wy0, ix[1], iy[1], xlf[1], ylf[1], F1);
         }
     }
 
@@ -931,7 +703,7 @@ k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, d
         sv[p][0] = sv[p][1] = sv[p][2] = sv[p][3] = 0;
         if (!live[p]) continue;
         const int64_t k = kk[p];
-        const float *Fp = p ? F1 : F0;
+        const FT *Fp = p ? F1 : F0;
         const double Ex = Fp[0], Ey = Fp[1], Ez = Fp[2], Bx = Fp[3], By = Fp[4], Bz = Fp[5];
         const double mk = m_a[k], qk = FIRST ? q_p[k] : q_f[k];
         const double opx = px_p[k], opy = py_p[k], opz = pz_p[k];
@@ -978,45 +750,79 @@ k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, d
         const double dro = qk / (1 - pz * igd);
         const double rg = dro * igd;
         const double djx = px * rg, djy = py * rg, djz = pz * rg;
-        check_range<fix_t>(dro, djx, djy, djz, ih, err);
-        const int c_x = cell_of((xi0 + xo) * ih + 0.5, half_n, dxl[p]);
-        const int c_y = cell_of((yi0 + yo) * ih + 0.5, half_n, dyl[p]);
+        if (MIXED) check_range<fix_t>(dro, djx, djy, djz, ih, err);
+        const int c_x = cell_of((MIXED ? (xi0 + xo) * ih : (xi0 + xo) / h) + 0.5, half_n, dxl[p]);
+        const int c_y = cell_of((MIXED ? (yi0 + yo) * ih : (yi0 + yo) / h) + 0.5, half_n, dyl[p]);
         if (!(c_x >= 2 && c_x < N - 2 && c_y >= 2 && c_y < N - 2)) {
             if (err) atomicOr(err, LCB_DEVERR_PLASMA_STENCIL);
             continue;
         }
         cx[p] = c_x; cy[p] = c_y;
-        const double sc = FIX_SCALE * ih * ih;
+        // mixed: values scaled to fixed-point units (with the 1/h^2 of the
+        // weights); FP64: the values themselves
+        const double sc = MIXED ? FIX_SCALE * ih * ih : 1.0;
         sv[p][0] = dro * sc; sv[p][1] = djx * sc; sv[p][2] = djy * sc; sv[p][3] = djz * sc;
     }
 
     // ---- phase 4: deposit ----
-    {
+    if constexpr (MIXED) {
+        {
+            const int lx = cx[0] - 2 - wx0, ly = cy[0] - 2 - wy0;
+            const bool joint = cx[0] >= 0 && cx[0] == cx[1] && cy[0] == cy[1] &&
+                               lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY &&
+                               shared_fix_ok(sv[0]) && shared_fix_ok(sv[1]);
+            if (joint) {
+                double ax[5], ay[5], bx[5], by[5];
+                weights4(dxl[0], ax); weights4(dyl[0], ay);
+                weights4(dxl[1], bx); weights4(dyl[1], by);
+#pragma unroll
+                for (int a = 0; a < 5; a++) {
+#pragma unroll
+                    for (int b = 0; b < 5; b++) {
+                        const double wa = ax[a] * ay[b], wb = bx[a] * by[b];
+                        const int c = (lx + a) * WY + ly + b;
+#pragma unroll
+                        for (int q = 0; q < 4; q++)
+                            shared_fix_add(swl, swh, q * WSZ + c,
+                                           fix_bits(fma(sv[0][q], wa, fma(sv[1][q], wb, FIX_MAGIC))));
+                    }
+                }
+            } else {
+                if (cx[0] >= 0)
+                    deposit_fix_one<WX, WY>(swl, swh, g4, N, wx0, wy0, cx[0], cy[0], dxl[0], dyl[0], sv[0]);
+                if (cx[1] >= 0)
+                    deposit_fix_one<WX, WY>(swl, swh, g4, N, wx0, wy0, cx[1], cy[1], dxl[1], dyl[1], sv[1]);
+            }
+        }
+    } else {
         const int lx = cx[0] - 2 - wx0, ly = cy[0] - 2 - wy0;
         const bool joint = cx[0] >= 0 && cx[0] == cx[1] && cy[0] == cy[1] &&
-                           lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY &&
-                           shared_fix_ok(sv[0]) && shared_fix_ok(sv[1]);
+                           lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY;
         if (joint) {
+            // the two contributions summed before one FP64 shared atomic
             double ax[5], ay[5], bx[5], by[5];
             weights4(dxl[0], ax); weights4(dyl[0], ay);
             weights4(dxl[1], bx); weights4(dyl[1], by);
 #pragma unroll
+            for (int b = 0; b < 5; b++) { ay[b] *= ih; by[b] *= ih; }
+#pragma unroll
             for (int a = 0; a < 5; a++) {
+                const double xa = ax[a] * ih, xb = bx[a] * ih;
 #pragma unroll
                 for (int b = 0; b < 5; b++) {
-                    const double wa = ax[a] * ay[b], wb = bx[a] * by[b];
+                    const double wa = xa * ay[b], wb = xb * by[b];
                     const int c = (lx + a) * WY + ly + b;
 #pragma unroll
                     for (int q = 0; q < 4; q++)
-                        shared_fix_add(swl, swh, q * WSZ + c,
-                                       fix_bits(fma(sv[0][q], wa, fma(sv[1][q], wb, FIX_MAGIC))));
+                        atomicAdd(sw + q * WSZ + c, fma(sv[0][q], wa, sv[1][q] * wb));
                 }
             }
         } else {
-            if (cx[0] >= 0)
-                deposit_fix_one<WX, WY>(swl, swh, g4, N, wx0, wy0, cx[0], cy[0], dxl[0], dyl[0], sv[0]);
-            if (cx[1] >= 0)
-                deposit_fix_one<WX, WY>(swl, swh, g4, N, wx0, wy0, cx[1], cy[1], dxl[1], dyl[1], sv[1]);
+#pragma unroll
+            for (int p = 0; p < 2; p++)
+                deposit_one<double, WX, WY>(reinterpret_cast<double *>(sw), g4[0], g4[1], g4[2], g4[3],
+                                            N, h, wx0, wy0, cx[p] >= 0, cx[p], cy[p], dxl[p], dyl[p],
+                                            sv[p][0], sv[p][1], sv[p][2], sv[p][3]);
         }
     }
     __syncthreads();
@@ -1026,49 +832,59 @@ k_move_deposit_mx(int64_t n_per_sort, int Ns, int N, double h, double xi_step, d
         const int64_t c = (int64_t)gx * N + gy;
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            const long long v = ((long long)swh[q * WSZ + t] << 20) + (long long)swl[q * WSZ + t];
-            if (v) atomicAdd(g4[q] + c, (fix_t)v);
+            if constexpr (MIXED) {
+                const long long v = ((long long)swh[q * WSZ + t] << 20) + (long long)swl[q * WSZ + t];
+                if (v) atomicAdd(g4[q] + c, (fix_t)v);
+            } else {
+                const double v = sw[q * WSZ + t];
+                if (v != 0.0) atomicAdd(g4[q] + c, v);
+            }
         }
     }
 }
 
-template <int WX, int WY>
-static size_t move_deposit_mx_smem()
+template <typename FT, int WX, int WY>
+static size_t move_deposit_pair_smem()
 {
-    return (size_t)WX * (FieldStride<WY>::v * 6 * sizeof(float) + WY * 4 * sizeof(fix_t));
+    return (size_t)WX * (FieldStride<WY, FT>::v * 6 * sizeof(FT) +
+                         WY * 4 * sizeof(typename StageAcc<FT>::type));
 }
 
-template <int WX, int WY, bool FIRST>
-static int launch_move_deposit_mx(const lcb_move_deposit_args *a, dim3 grid, fix_t *w,
-                                  size_t plane, cudaStream_t st)
+template <typename FT, int WX, int WY, bool FIRST>
+static int launch_move_deposit_pair(const lcb_move_deposit_args *a, dim3 grid,
+                                    typename StageAcc<FT>::type *const out[4], cudaStream_t st)
 {
-    const size_t sm = move_deposit_mx_smem<WX, WY>();
+    const size_t sm = move_deposit_pair_smem<FT, WX, WY>();
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_move_deposit_mx<WX, WY, FIRST>,
+        cudaError_t e = cudaFuncSetAttribute(k_move_deposit_pair<FT, WX, WY, FIRST>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return cuda_check(e, "move_deposit smem attribute");
         attr = true;
     }
     const lcb_plasma_particles &p = a->prev, &f = a->full;
-    k_move_deposit_mx<WX, WY, FIRST><<<grid, DEP_THREADS, sm, st>>>(
+    k_move_deposit_pair<FT, WX, WY, FIRST><<<grid, DEP_THREADS, sm, st>>>(
         a->n_per_sort, a->particles_side, a->grid_steps, a->h, a->xi_step, a->boundary,
         a->fields[0], a->fields[1], a->fields[2], a->fields[3], a->fields[4], a->fields[5],
         p.x_init, p.y_init, p.x_offt, p.y_offt, p.px, p.py, p.pz, p.q, p.m,
-        f.q, f.x_offt, f.y_offt, f.px, f.py, f.pz, w, w + 2 * plane, w + 4 * plane,
-        w + 6 * plane, a->err);
+        f.q, f.x_offt, f.y_offt, f.px, f.py, f.pz, out[0], out[1], out[2], out[3], a->err);
     return LCB_OK;
 }
 
-static int dispatch_move_deposit_mx(const lcb_move_deposit_args *a, dim3 grid, fix_t *w,
-                                    size_t plane, cudaStream_t st)
+// Window: the tile's cells (8 x 16 with two or more particles per cell,
+// 16 x 32 with one) + 2 stencil + 4 slack on each side.
+template <typename FT>
+static int dispatch_move_deposit_pair(const lcb_move_deposit_args *a,
+                                      typename StageAcc<FT>::type *const out[4], cudaStream_t st)
 {
-    grid.y = (a->particles_side + 1 + DEP_TI - 1) / DEP_TI;  // spare row of tiles
+    const dim3 grid((a->particles_side + DEP_TJ - 1) / DEP_TJ,
+                    (a->particles_side + 1 + DEP_TI - 1) / DEP_TI,   // spare tile row
+                    a->n_sorts);
     if (a->lattice_fineness >= 2)
-        return a->first ? launch_move_deposit_mx<20, 28, true>(a, grid, w, plane, st)
-                        : launch_move_deposit_mx<20, 28, false>(a, grid, w, plane, st);
-    return a->first ? launch_move_deposit_mx<DEP_WX, DEP_WY, true>(a, grid, w, plane, st)
-                    : launch_move_deposit_mx<DEP_WX, DEP_WY, false>(a, grid, w, plane, st);
+        return a->first ? launch_move_deposit_pair<FT, 20, 28, true>(a, grid, out, st)
+                        : launch_move_deposit_pair<FT, 20, 28, false>(a, grid, out, st);
+    return a->first ? launch_move_deposit_pair<FT, DEP_WX, DEP_WY, true>(a, grid, out, st)
+                    : launch_move_deposit_pair<FT, DEP_WX, DEP_WY, false>(a, grid, out, st);
 }
 
 // Fixed-point sums (4 quantities x 2 columns x N*N) to the FP64 outputs;
@@ -1250,8 +1066,6 @@ extern "C" int lcb_plasma_move_deposit(const lcb_move_deposit_args *a, void *str
     for (int f = 0; f < 6; f++) LCB_REQUIRE(a->fields[f], "field plane %d is NULL", f);
     cudaStream_t st = as_stream(stream);
     const size_t plane = (size_t)N * N;
-    const dim3 grid((a->particles_side + DEP_TJ - 1) / DEP_TJ,
-                    (a->particles_side + DEP_TI - 1) / DEP_TI, a->n_sorts);
     if (a->precision == LCB_PREC_MIXED) {
         LCB_REQUIRE(a->workspace && a->workspace_bytes >= lcb_plasma_deposit_workspace_bytes(N, a->precision),
                     "deposit workspace too small");
@@ -1259,9 +1073,10 @@ extern "C" int lcb_plasma_move_deposit(const lcb_move_deposit_args *a, void *str
         cudaError_t e = cudaMemsetAsync(w, 0, 8 * plane * sizeof(fix_t), st);
         if (e != cudaSuccess) return cuda_check(e, "memset fixed-point sums");
         if (a->n_per_sort > 0) {
-            const int rc = dispatch_move_deposit_mx(a, grid, w, plane, st);
+            fix_t *const out[4] = {w, w + 2 * plane, w + 4 * plane, w + 6 * plane};
+            const int rc = dispatch_move_deposit_pair<float>(a, out, st);
             if (rc) return rc;
-            LCB_LAUNCH_CHECK("k_move_deposit_mx");
+            LCB_LAUNCH_CHECK("k_move_deposit_pair<float>");
         }
         k_fix_finish<<<grid_for(2 * plane, 256), 256, 0, st>>>(
             plane, a->n_sorts, w, a->ro_initial, a->ro, a->jx, a->jy, a->jz);
@@ -1273,9 +1088,10 @@ extern "C" int lcb_plasma_move_deposit(const lcb_move_deposit_args *a, void *str
         if (e != cudaSuccess) return cuda_check(e, "memset currents");
     }
     if (a->n_per_sort > 0) {
-        const int rc = dispatch_move_deposit<double>(a, grid, a->ro, a->jx, a->jy, a->jz, st);
+        double *const out[4] = {a->ro, a->jx, a->jy, a->jz};
+        const int rc = dispatch_move_deposit_pair<double>(a, out, st);
         if (rc) return rc;
-        LCB_LAUNCH_CHECK("k_move_deposit<double>");
+        LCB_LAUNCH_CHECK("k_move_deposit_pair<double>");
     }
     if (a->ro_initial) {
         cudaError_t e = cudaMemcpyAsync(a->ro + plane, a->ro_initial, plane * sizeof(double),

@@ -97,10 +97,11 @@ class Plane2d3vPlasmaSolver:
         # planes are copied into fixed buffers so the graphs stay valid.
         pe = config.getraw('cuda-graphs')
         self.use_graphs = True if pe is None else bool(pe)
-        # one fused kernel per predictor-corrector stage (move + deposit):
-        # faster with FP32 accumulation; in FP64 the separate kernels win
+        # one fused kernel per predictor-corrector stage (K1/K2 + K3), the
+        # default in both precisions; 'fused-particle-kernels': False runs
+        # the three reference kernels separately
         pf = config.getraw('fused-particle-kernels')
-        self.fused = (self.dep_precision == _lib.LCB_PREC_MIXED) if pf is None else bool(pf)
+        self.fused = True if pf is None else bool(pf)
         self.fineness = max(1, int(round(config.getfloat('plasma-fineness') or 1)))
         self.rbf = torch.zeros(N, N, dtype=torch.float64, device=dev)
         self.rbp = torch.zeros(N, N, dtype=torch.float64, device=dev)
