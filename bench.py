@@ -655,9 +655,10 @@ def main():
 
 # DRAM bytes (read + written) per call of the dominant op, from one ncu
 # capture of the small case of the same workload (N=513, 11 xi steps):
-# compute_fields in FP64 counts its four DMMA waves, move_deposit the fused
+# compute_fields counts its four tensor-core waves, move_deposit the fused
 # kernel of a non-first stage.
-NCU_TRAFFIC = {("compute_fields", "fp64"): 77.8e6, ("move_deposit", "mixed"): 116.0e6}
+NCU_TRAFFIC = {("compute_fields", "fp64"): 85.5e6, ("compute_fields", "mixed"): 43.6e6,
+               ("move_deposit", "fp64"): 119.5e6, ("move_deposit", "mixed"): 116.7e6}
 
 
 def transform_flops(N):
@@ -685,17 +686,14 @@ def roofline(r, N, hbm_peak, peak_src, peaks):
     o = ops[name]
     Np = 964 * 964
     if name == "compute_fields":
-        flops = transform_flops(N)
-        if r.get("precision", "fp64") == "fp64":
-            achieved = flops / (o["ms_avg"] / 1e3) / 1e12
-            return {"bound": "tensor", "kernel": name + " (FP64 DMMA waves)", "achieved": achieved,
-                    "peak": 37.0, "unit": "TFLOP/s", "frac": achieved / 37.0,
-                    "traffic": NCU_TRAFFIC.get((name, "fp64")),
-                    "peak_source": "nominal B200 FP64 tensor (no measured FP64 peak on this pool)"}
-        # mixed: ten int8 slice products per FP32 product
-        achieved = 10 * flops / (o["ms_avg"] / 1e3) / 1e12
-        return {"bound": "tensor", "kernel": name + " (int8 tcgen05 waves)", "achieved": achieved,
-                "peak": 4500.0, "unit": "TOP/s", "frac": achieved / 4500.0, "traffic": None,
+        # executed int8 operations: one slice-pair product per pair i + j < NS
+        prec = r.get("precision", "fp64")
+        ns = 8 if prec == "fp64" else 4
+        ops_int8 = ns * (ns + 1) // 2 * transform_flops(N)
+        achieved = ops_int8 / (o["ms_avg"] / 1e3) / 1e12
+        return {"bound": "tensor", "kernel": name + f" (int8 tcgen05 waves, {ns} slices)",
+                "achieved": achieved, "peak": 4500.0, "unit": "TOP/s", "frac": achieved / 4500.0,
+                "traffic": NCU_TRAFFIC.get((name, prec)),
                 "peak_source": "nominal B200 dense int8 (no measured int8 peak on this pool)"}
     per = {"deposit": 72, "move_smart": 128, "move_wo_fields": 64,
            "move_deposit": 128 + 72}.get(name, 0)
