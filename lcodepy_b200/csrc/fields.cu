@@ -443,10 +443,12 @@ __device__ __forceinline__ double epi_apply(const GemmBatch<T> &b, const GemmDes
 
 template <int NS, int BN>
 struct I8Cfg {
-    static_assert(BN == TL_N, "B tiles are 64 wide");
-    static constexpr int ST = 4;                                       // pipeline stages
+    // a CTA covers BN columns: a whole 64-wide B tile or, for BN = 32, the
+    // contiguous half of one (its N core-matrix groups 0-1 or 2-3)
+    static_assert(TL_N % BN == 0 && BN % 16 == 0, "tile width");
     static constexpr int B_SLICE = I8_BK * BN;                         // bytes
     static constexpr int STAGE = NS * (I8_A_SLICE + B_SLICE);          // bytes
+    static constexpr int ST = 4 * STAGE <= 100 * 1024 ? 4 : 2;         // pipeline stages
     static constexpr int TMEM_COLS = NS * BN;                          // power of two
     static constexpr size_t smem = (size_t)ST * STAGE + 128;   // + 2 ST + 1 barriers, TMEM slot
 };
@@ -465,7 +467,7 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
     using Cfg = I8Cfg<NS, BN>;
     constexpr int ST = Cfg::ST;
     static_assert(Cfg::TMEM_COLS == 256 || Cfg::TMEM_COLS == 512, "tensor memory columns");
-    static_assert(8 * 32 * 33 * sizeof(T) <= (size_t)ST * Cfg::STAGE, "epilogue staging");
+    static_assert(8 * 32 * (BN / 2 + 1) * sizeof(T) <= (size_t)ST * Cfg::STAGE, "epilogue staging");
     extern __shared__ __align__(1024) uint8_t i8sm[];
     uint64_t *full = reinterpret_cast<uint64_t *>(i8sm + ST * Cfg::STAGE);   // [ST] copies landed
     uint64_t *done = full + ST;                                             // [ST] MMAs finished
@@ -481,7 +483,8 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
     const int KT = ntiles(K, TL_K);
     // this CTA's tile rows of A and tile column of B
     const uint8_t *At = reinterpret_cast<const uint8_t *>(g.A) + (int64_t)blockIdx.y * KT * I8_A_SLICE;
-    const uint8_t *Bt = reinterpret_cast<const uint8_t *>(g.B) + (int64_t)blockIdx.x * KT * Cfg::B_SLICE;
+    const uint8_t *Bt = reinterpret_cast<const uint8_t *>(g.B) + (int64_t)(n0 / TL_N) * KT * (TL_K * TL_N) +
+                        ((n0 % TL_N) >> 4) * 512;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -515,7 +518,7 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
             for (int i = 0; i < NS; i++) {
                 bulk_g2s(sA + i * I8_A_SLICE, At + (int64_t)i * g.a_plane + (int64_t)kt * I8_A_SLICE,
                          I8_A_SLICE, mb);
-                bulk_g2s(sB + i * Cfg::B_SLICE, Bt + (int64_t)i * g.b_plane + (int64_t)kt * Cfg::B_SLICE,
+                bulk_g2s(sB + i * Cfg::B_SLICE, Bt + (int64_t)i * g.b_plane + (int64_t)kt * (TL_K * TL_N),
                          Cfg::B_SLICE, mb);
             }
         };
@@ -568,15 +571,16 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
     // |.| < 2^53), with one conversion per four; the values go through shared
     // memory (the pipeline buffers are free now) so that the stores run along
     // rows
+    constexpr int CW = BN / 2;            // columns per warp
     const int rq = warp & 3, ch = warp >> 2;
-    T *stage = reinterpret_cast<T *>(i8sm) + warp * 32 * 33;
+    T *stage = reinterpret_cast<T *>(i8sm) + warp * 32 * (CW + 1);
     const double scale = ldexp(1.0, ea + eb - 33);
 #pragma unroll 1
-    for (int c8 = 0; c8 < 4; c8++) {
+    for (int c8 = 0; c8 < CW / 8; c8++) {
         unsigned r[NS][8];
 #pragma unroll
         for (int q = 0; q < NS; q++) {
-            const unsigned taddr = tmem + ((unsigned)(32 * rq) << 16) + (unsigned)(q * BN + 32 * ch + 8 * c8);
+            const unsigned taddr = tmem + ((unsigned)(32 * rq) << 16) + (unsigned)(q * BN + CW * ch + 8 * c8);
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                          : "=r"(r[q][0]), "=r"(r[q][1]), "=r"(r[q][2]), "=r"(r[q][3]),
                            "=r"(r[q][4]), "=r"(r[q][5]), "=r"(r[q][6]), "=r"(r[q][7])
@@ -596,27 +600,30 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
                                      ((long long)(int)r[6][e] << 7) + (long long)(int)r[7][e];
                 v = (T)(((double)c + ldexp((double)c2, -28)) * scale);
             }
-            stage[lane * 33 + 8 * c8 + e] = ok ? v : (T)__int_as_float(0x7fc00000);
+            stage[lane * (CW + 1) + 8 * c8 + e] = ok ? v : (T)__int_as_float(0x7fc00000);
         }
     }
     __syncwarp();
     double part = 0;
     float vmax = 0.f;
-    // rows in groups of 8: the scale factors or previous fields they need
-    // are loaded for the whole group before any store
+    // the warp's 32 x CW values, 32 per pass with lanes along a row; passes
+    // in groups of 8, whose scale factors or previous fields are loaded
+    // before any store
 #pragma unroll 1
-    for (int r0 = 0; r0 < 32; r0 += 8) {
+    for (int it0 = 0; it0 < CW; it0 += 8) {
         double pre[8];
 #pragma unroll
-        for (int rr = 0; rr < 8; rr++) {
-            const int gm = m0 + 32 * rq + r0 + rr, gn = n0 + 32 * ch + lane;
-            pre[rr] = (gm < M && gn < N) ? epi_pre<EPI, T>(batch, g, gm, gn) : 0.0;
+        for (int u = 0; u < 8; u++) {
+            const int e = (it0 + u) * 32 + lane, row = e / CW, col = e % CW;
+            const int gm = m0 + 32 * rq + row, gn = n0 + CW * ch + col;
+            pre[u] = (gm < M && gn < N) ? epi_pre<EPI, T>(batch, g, gm, gn) : 0.0;
         }
 #pragma unroll
-        for (int rr = 0; rr < 8; rr++) {
-            const int gm = m0 + 32 * rq + r0 + rr, gn = n0 + 32 * ch + lane;
+        for (int u = 0; u < 8; u++) {
+            const int e = (it0 + u) * 32 + lane, row = e / CW, col = e % CW;
+            const int gm = m0 + 32 * rq + row, gn = n0 + CW * ch + col;
             if (gm >= M || gn >= N) continue;
-            part += epi_apply<EPI, T>(batch, g, gm, gn, stage[(r0 + rr) * 33 + lane], pre[rr], vmax);
+            part += epi_apply<EPI, T>(batch, g, gm, gn, stage[row * (CW + 1) + col], pre[u], vmax);
         }
     }
     if (EPI != EPI_FIELD && batch.amax_out) {
@@ -977,7 +984,9 @@ static Work<T> carve(void *ws, int N)
 template <typename T, int EPI>
 static int launch_i8(const GemmBatch<T> &b, int nsub, int maxM, int maxN, cudaStream_t st)
 {
-    constexpr int BN = 64;
+    // 256 tensor-memory columns per CTA (NS accumulators x BN) so that two
+    // CTAs share an SM: 64-wide tiles for four slices, 32-wide for eight
+    constexpr int BN = Slices<T>::n == 8 ? 32 : 64;
     using Cfg = I8Cfg<Slices<T>::n, BN>;
     static bool attr = false;
     if (!attr) {
