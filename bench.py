@@ -53,27 +53,10 @@ def workload_config(precision="fp64", window_length=60.0):
 def make_beam(n=1_000_000, seed=2024, sigma_r=0.5, sigma_z=1.0, xi0=-3.0,
               gamma=1000.0, espread=0.01, emittance=1e-2, peak=-0.5, dxi=0.02,
               r_max=4.0):
-    """Seeded bi-Gaussian driver as a particle_dtype3d array.  q_norm makes the
-    deposited on-axis peak density equal `peak` (layer charge per cell area):
-    rho = Q dxi / (sqrt(2 pi) sigma_z) / (2 pi sigma_r^2)."""
-    from lcodepy_b200.beam_generator import particle_dtype3d
-    rng = np.random.default_rng(seed)
-    xi = rng.normal(xi0, sigma_z, 2 * n)
-    xi = xi[(xi < 0) & (xi > 2 * xi0)][:n]
-    m = xi.size
-    r = sigma_r * np.sqrt(-2 * np.log(1 - rng.random(m) * (1 - np.exp(-r_max ** 2 / (2 * sigma_r ** 2)))))
-    phi = rng.uniform(0, 2 * np.pi, m)
-    b = np.zeros(m, dtype=particle_dtype3d)
-    b['xi'] = xi
-    b['x'], b['y'] = r * np.cos(phi), r * np.sin(phi)
-    sp = emittance / sigma_r
-    b['px'], b['py'] = rng.normal(0, sp, m), rng.normal(0, sp, m)
-    b['pz'] = rng.normal(gamma, gamma * espread, m)
-    b['q_m'] = -1.0
-    q_total = peak * (np.sqrt(2 * np.pi) * sigma_z) * (2 * np.pi * sigma_r ** 2) / dxi
-    b['q_norm'] = q_total / m
-    b['id'] = np.arange(1, m + 1)
-    return b[np.argsort(-b['xi'])]
+    """The workload's seeded bi-Gaussian driver (a particle_dtype3d array)."""
+    from lcodepy_b200.batch import bigaussian_beam
+    return bigaussian_beam(n, seed, sigma_r, sigma_z, xi0, gamma, espread, emittance, peak,
+                           dxi, r_max)
 
 
 class ClockSampler:
@@ -286,12 +269,12 @@ def run_batch(args, ws, rank, local):
     the on-axis Ez error."""
     import torch
     from lcodepy_b200 import Simulation
-    from lcodepy_b200.batch import BatchRunner, Member, scan_members
+    from lcodepy_b200.batch import BatchRunner, make_member, scan_members
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     W, K = args.warmup, args.steps
     specs = scan_members(n=args.members, n_steps=W + K, precision=args.precision)
-    members = [Member(c, d, dev) for c, d in specs]
+    members = [make_member(c, d, dev) for c, d in specs]
     runner = BatchRunner(members)
     for _ in range(W):
         runner.step()
@@ -353,26 +336,37 @@ def run_batch(args, ws, rank, local):
             "clocks": clocks, "cells": cells, "members": len(specs), "launches": launches}
 
 
-def plain_ms_per_step(N, precision="fp64", n_steps=120, skip=20):
-    """Device ms per xi step of the plain drop-in path (Simulation, default
-    settings) on an N x N rigid-driver grid at h = dxi = 0.05."""
+def plain_ms_per_step(N, precision="fp64", n_steps=120, skip=20, beam=None):
+    """Device ms per xi step of the plain drop-in path (PusherAndSolver3D
+    with default settings) on an N x N grid at h = dxi = 0.05, with a rigid
+    Gaussian driver or the given BeamDriver."""
     import torch
-    from lcodepy_b200 import Simulation
     from lcodepy_b200.batch import GaussianDriver, request_stream
-    cfg = dict(request_stream(n=1, sizes=(N,), min_steps=n_steps, max_steps=n_steps)[0][2])
+    from lcodepy_b200.beam3d import BeamDrain, BeamSource, RigidBeamSource
+    from lcodepy_b200.config import Config
+    from lcodepy_b200.push_solver import PusherAndSolver3D
+    cfg = dict(request_stream(n=1, sizes=(N,), min_steps=n_steps, max_steps=n_steps,
+                              beam_fraction=0.0)[0][2])
     cfg['precision'] = precision
-    sim = Simulation(config=cfg, beam_parameters=GaussianDriver(), runas_filename='')
-    ps = sim.push_solver
+    cfg['rigid-beam'] = beam is None
+    conf = Config(cfg)
+    conf._adjust_config_values_3d()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    ps = PusherAndSolver3D(conf, dev)
     ev = {}
 
     def hook(k):
         if k in (skip, n_steps):
             ev[k] = torch.cuda.Event(enable_timing=True)
             ev[k].record()
-    from lcodepy_b200.beam3d import RigidBeamSource
     ps.plasma_solver.init_state(1.0)
-    ps.step_dt(cfg['xi-step'], RigidBeamSource(None, GaussianDriver()), None, 1.0, [],
-               step_hook=hook)
+    if beam is None:
+        src, drain = RigidBeamSource(None, GaussianDriver()), None
+    else:
+        import dataclasses
+        beam = dataclasses.replace(beam, r_max=min(beam.r_max, 0.4 * cfg['window-width']))
+        src, drain = BeamSource(conf, beam.particles(cfg['xi-step']), dev), BeamDrain(conf, dev)
+    ps.step_dt(cfg['xi-step'], src, drain, 1.0, [], step_hook=hook)
     torch.cuda.synchronize()
     return ev[skip].elapsed_time(ev[n_steps]) / (n_steps - skip)
 
@@ -380,7 +374,8 @@ def plain_ms_per_step(N, precision="fp64", n_steps=120, skip=20):
 def run_serve(args, ws, rank, local):
     """The served stream: requests with Poisson arrivals (20 per second,
     seeded), grids 129/257/513 at h = 0.05, xi lengths uniform in 200..2000
-    steps of 0.05, rigid Gaussian drivers; admitted by HBM footprint into at
+    steps of 0.05, half of the drivers rigid Gaussians and half non-rigid
+    bi-Gaussian beams of 100k..1M macroparticles; admitted by HBM footprint into at
     most --slots concurrent members, each advanced by captured graphs on its
     own stream.  The plain comparison runs the same requests one by one, first
     come first served, through the plain FP64 drop-in path; its per-step cost
@@ -395,9 +390,11 @@ def run_serve(args, ws, rank, local):
     # warm the library, the allocator and the graph path on a short request
     warm = Server(hbm_budget_bytes=args.hbm_budget_gb << 30, max_slots=args.slots, device=dev)
     for N in (129, 257, 513):
-        c = dict(request_stream(n=1, sizes=(N,), min_steps=8, max_steps=8,
-                                precision=args.precision)[0][2])
-        warm.submit(f"warm{N}", c, reqs[0][3], arrival=0.0)
+        for bf in (0.0, 1.0):
+            _, _, c, d = request_stream(n=1, sizes=(N,), min_steps=8, max_steps=8,
+                                        precision=args.precision, beam_fraction=bf,
+                                        beam_particles=(50_000, 50_000))[0]
+            warm.submit(f"warm{N}{bf}", c, d, arrival=0.0)
     warm.run()
     torch.cuda.synchronize()
     barrier(ws)
@@ -422,13 +419,19 @@ def run_serve(args, ws, rank, local):
     cell_steps = sum(d["cells"] * d["steps"] for d in done.values())
     lat = np.array([done[r]["latency"] for _, r, _, _ in reqs])
     value = ws * cell_steps / (ms / 1e3)
-    # plain path, request by request, first come first served
+    # plain path, request by request, first come first served: per-step cost
+    # per grid size, measured with a rigid driver and with a beam of the mean
+    # size (550k macroparticles)
+    from lcodepy_b200.batch import BeamDriver
     per = {N: plain_ms_per_step(N) for N in (129, 257, 513)}
+    per_beam = ({N: plain_ms_per_step(N, beam=BeamDriver(n=550_000, amplitude=0.1))
+                 for N in (129, 257, 513)}
+                if any(isinstance(r[3], BeamDriver) for r in reqs) else per)
     finish, plain_lat, busy = 0.0, [], 0.0
     for arr, rid, cfg, drv in reqs:
         d = done[rid]
         N = int(round(math.sqrt(d["cells"])))
-        dur = d["steps"] * per[N] / 1e3
+        dur = d["steps"] * (per_beam if isinstance(drv, BeamDriver) else per)[N] / 1e3
         finish = max(finish, arr) + dur
         busy += dur
         plain_lat.append(finish - arr)
@@ -437,19 +440,17 @@ def run_serve(args, ws, rank, local):
     # accuracy: a few requests rerun alone through the plain FP64 path
     errs = []
     if args.check_requests:
-        from lcodepy_b200 import Simulation
+        from lcodepy_b200.batch import solo_ez
         for arr, rid, cfg, drv in sorted(reqs, key=lambda r: r[2]['window-length'])[
                 :args.check_requests]:
-            sim = Simulation(config={**cfg, 'precision': 'fp64'}, beam_parameters=drv,
-                             runas_filename='')
-            sim.step()
-            ez64 = sim.push_solver.ez_axis.cpu().numpy()
+            ez64 = solo_ez(cfg, drv, precision='fp64')
             errs.append(float(np.linalg.norm(done[rid]["ez"] - ez64) / np.linalg.norm(ez64)))
-            del sim
     return {"value": value, "ms": ms, "wall_s": wall, "cell_steps": cell_steps,
             "p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
             "plain_value": plain_value, "plain_p50": float(np.percentile(plain_lat, 50)),
             "plain_p99": float(np.percentile(plain_lat, 99)), "plain_ms_per_step": per,
+            "plain_ms_per_step_beam": per_beam,
+            "beam_requests": sum(isinstance(r[3], BeamDriver) for r in reqs),
             "errs": errs, "clocks": clocks, "launches": launches,
             "span_arrivals_s": reqs[-1][0]}
 
@@ -580,10 +581,13 @@ def main():
                 "ms_per_step": r["ms"] / args.requests,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "mixed" if args.precision == "mixed" else "f64",
-                "data": "synthetic (seeded Poisson request stream, rigid Gaussian drivers)",
+                "data": "synthetic (seeded Poisson request stream; rigid Gaussian and "
+                        "seeded bi-Gaussian beam drivers)",
                 "config": {"workload": f"served stream: {args.requests} requests, Poisson "
                                        "20/s, grids 129/257/513 at h=0.05, 200-2000 xi "
-                                       "steps of 0.05, ppc=4",
+                                       "steps of 0.05, ppc=4, drivers half rigid, half "
+                                       "beams of 100k-1M macroparticles",
+                           "beam_requests": r["beam_requests"],
                            "precision": args.precision, "slots": args.slots,
                            "hbm_budget_gb": args.hbm_budget_gb,
                            "steps_are": "requests; ms_per_step = makespan / requests",
@@ -592,7 +596,8 @@ def main():
                 "makespan_s": r["ms"] / 1e3, "cell_steps": r["cell_steps"],
                 "plain_fp64": {"value": r["plain_value"], "p50": r["plain_p50"],
                                "p99": r["plain_p99"],
-                               "ms_per_step": r["plain_ms_per_step"]},
+                               "ms_per_step": r["plain_ms_per_step"],
+                               "ms_per_step_beam": r["plain_ms_per_step_beam"]},
                 "served_vs_plain": r["value"] / r["plain_value"],
                 "ez_rel_l2_vs_fp64": r["errs"],
                 "gpu_launches": r["launches"], "clocks": r["clocks"]}), flush=True)

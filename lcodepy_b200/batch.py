@@ -1,13 +1,17 @@
 """Many simulations on one GPU: batched parameter scans and a served request
 stream.
 
-Each ``Member`` is one quasistatic 3D simulation with a rigid Gaussian driver
-(the driver family of the benchmark configurations).  Its whole xi step --
-driver evaluated on the device from a step counter, predictor-corrector
-plasma step, on-axis Ez record -- is captured once in two CUDA graphs (one
-per parity of the rotating buffers) and replayed on the member's own stream,
-so members of any grid size advance concurrently and a host loop only issues
-one graph launch per member and xi step.
+Each ``Member`` is one quasistatic 3D simulation with a rigid Gaussian driver.
+Its whole xi step -- driver evaluated on the device from a step counter,
+predictor-corrector plasma step, on-axis Ez record -- is captured once in two
+CUDA graphs (one per parity of the rotating buffers) and replayed on the
+member's own stream, so members of any grid size advance concurrently and a
+host loop only issues one graph launch per member and xi step.
+
+A ``BeamMember`` has a non-rigid driver (macroparticles of a bi-Gaussian
+beam): its plasma step is the same captured graph, and the beam layer step
+(push, ordered compaction, layout of the next layer, with device counters)
+is launched beside it on the member's stream, without host round trips.
 
 ``BatchRunner`` advances a fixed set of members together (a parameter scan).
 ``Server`` admits requests that arrive over time into free slots while others
@@ -47,7 +51,61 @@ class GaussianDriver:
         return xp.zeros_like(x)
 
 
-def footprint_bytes(config: dict) -> int:
+@dataclasses.dataclass
+class BeamDriver:
+    """A non-rigid electron driver: n macroparticles, bi-Gaussian (sigma_r,
+    sigma_z) around xi0, peak density `amplitude` (in n0; the beam charge is
+    negative), gamma with a relative spread, normalised emittance; seeded."""
+    n: int = 100_000
+    amplitude: float = 0.1
+    sigma_r: float = 1.0
+    sigma_z: float = 1.0
+    xi0: float = -3.0
+    gamma: float = 1000.0
+    espread: float = 0.01
+    emittance: float = 1e-2
+    seed: int = 0
+    r_max: float = 4.0        # radial cut (keep it inside the window)
+
+    def particles(self, dxi: float) -> np.ndarray:
+        return bigaussian_beam(self.n, self.seed, self.sigma_r, self.sigma_z, self.xi0,
+                               self.gamma, self.espread, self.emittance, -self.amplitude, dxi,
+                               self.r_max)
+
+
+def bigaussian_beam(n=1_000_000, seed=2024, sigma_r=0.5, sigma_z=1.0, xi0=-3.0,
+                    gamma=1000.0, espread=0.01, emittance=1e-2, peak=-0.5, dxi=0.02,
+                    r_max=4.0) -> np.ndarray:
+    """Seeded bi-Gaussian beam as a particle_dtype3d array, sorted by xi
+    (descending), cut to xi in (2 xi0, 0) and r < r_max.  q_norm makes the
+    deposited on-axis peak density equal `peak` (layer charge per cell area):
+    rho = Q dxi / (sqrt(2 pi) sigma_z) / (2 pi sigma_r^2)."""
+    from .beam_generator import particle_dtype3d
+    rng = np.random.default_rng(seed)
+    xi = rng.normal(xi0, sigma_z, 2 * n)
+    xi = xi[(xi < 0) & (xi > 2 * xi0)][:n]
+    m = xi.size
+    r = sigma_r * np.sqrt(-2 * np.log(1 - rng.random(m) * (1 - np.exp(-r_max ** 2 / (2 * sigma_r ** 2)))))
+    phi = rng.uniform(0, 2 * np.pi, m)
+    b = np.zeros(m, dtype=particle_dtype3d)
+    b['xi'] = xi
+    b['x'], b['y'] = r * np.cos(phi), r * np.sin(phi)
+    sp = emittance / sigma_r
+    b['px'], b['py'] = rng.normal(0, sp, m), rng.normal(0, sp, m)
+    b['pz'] = rng.normal(gamma, gamma * espread, m)
+    b['q_m'] = -1.0
+    q_total = peak * (np.sqrt(2 * np.pi) * sigma_z) * (2 * np.pi * sigma_r ** 2) / dxi
+    b['q_norm'] = q_total / m
+    b['id'] = np.arange(1, m + 1)
+    return b[np.argsort(-b['xi'], kind='stable')]
+
+
+# device bytes per beam macroparticle: the sorted source, the drain, the two
+# fell-through buffers and the lost buffer (11 eight-byte fields each)
+BEAM_BYTES_PER_PARTICLE = 5 * 11 * 8
+
+
+def footprint_bytes(config: dict, driver=None) -> int:
     """Device memory one member needs (particles, fields, currents, solver
     workspaces), for admission decisions."""
     cfg = Config(config)
@@ -61,7 +119,8 @@ def footprint_bytes(config: dict) -> int:
     prec = _lib.LCB_PREC_MIXED if mixed else _lib.LCB_PREC_FP64
     particles = 2 * 9 * 8 * sorts * Ns * Ns
     planes = (4 * 7 + 2 * 4 * 2 + 4) * 8 * N * N
-    return int(particles + planes + L.lcb_compute_fields_workspace_bytes(N, prec)
+    beam = BEAM_BYTES_PER_PARTICLE * driver.n if isinstance(driver, BeamDriver) else 0
+    return int(particles + planes + beam + L.lcb_compute_fields_workspace_bytes(N, prec)
                + L.lcb_field_operators_bytes(N, prec)
                + L.lcb_plasma_deposit_workspace_bytes(N, prec) + (8 << 20))
 
@@ -157,8 +216,10 @@ class Member:
         return self.end_event is not None and self.end_event.query()
 
     def result(self):
-        """On-axis Ez per xi step and the final fields (host arrays)."""
+        """On-axis Ez per xi step and the final fields (host arrays); raises if
+        a kernel set a bit of the device error word."""
         self.stream.synchronize()
+        self.solver.check_errors()
         return {"ez": self.ez.cpu().numpy(),
                 "fields": self.solver.prev_fields.buf.cpu().numpy()}
 
@@ -166,6 +227,106 @@ class Member:
         self.graphs = [None, None]
         self.solver = None
         self.marks.clear()
+
+
+class BeamMember(Member):
+    """One simulation with a non-rigid driver.  Its plasma step is the
+    solver's captured graph (one per buffer parity); the beam layer step
+    (push of layer i - 1 between the previous and the new fields, layout of
+    layer i + 1, all on the device) and the on-axis Ez record are launched
+    around it on the member's stream."""
+
+    def __init__(self, config: dict, driver: BeamDriver, device=None, name=None):
+        from .beam3d import BeamCalculator, BeamSource
+        self.device = device or torch.device("cuda", torch.cuda.current_device())
+        cfg = Config(config)
+        cfg._adjust_config_values_3d()
+        self.config = cfg
+        self.name = name
+        self.driver = driver
+        self.N = cfg.getint('window-width-steps')
+        self.dxi = cfg.getfloat('xi-step')
+        self.n_steps = round(cfg.getfloat('window-length') / self.dxi) + 1
+        self.cells = self.N * self.N
+        self.stream = torch.cuda.Stream(self.device)
+        with torch.cuda.stream(self.stream):
+            self.solver = Plane2d3vPlasmaSolver(cfg, self.device)
+            self.solver.init_state(cfg.getfloat('time-step'))
+            self.solver.capture_on_stream = True
+            self.bc = BeamCalculator(cfg, self.device)
+            self.source = BeamSource(cfg, driver.particles(self.dxi), self.device)
+            self.bc.start_time_step(self.source)
+            self.bc.layout_first(0)
+            self.counter = torch.zeros(1, dtype=torch.int64, device=self.device)
+            self.ez = torch.zeros(self.n_steps, dtype=torch.float64, device=self.device)
+        self.done = 0
+        self.marks = collections.deque()
+        self.end_event = None
+        self.t_admit = None
+
+    def step(self):
+        if len(self.marks) >= self.MAX_AHEAD:
+            self.marks.popleft().synchronize()
+        ps, bc, i = self.solver, self.bc, self.done
+        L = _lib.load()
+        with torch.cuda.stream(self.stream):
+            rb_full, rb_prev = bc.rho(i)
+            ps.step_dxi(rb_full, rb_prev, bc.rho_divisor)
+            bc.after_plasma_step(i, ps.last_fields, ps.prev_fields)
+            _lib.check(L.lcb_record_axis(ps.prev_fields.Ez.data_ptr(), self.N,
+                                         self.counter.data_ptr(), self.ez.data_ptr(),
+                                         self.n_steps, _lib.stream_handle()), "lcb_record_axis")
+            self.done += 1
+            if self.done % self.MARK_EVERY == 0 or self.done >= self.n_steps:
+                ev = torch.cuda.Event()
+                ev.record(self.stream)
+                self.marks.append(ev)
+                if self.done >= self.n_steps:
+                    self.end_event = ev
+
+    def result(self):
+        out = super().result()
+        e = int(self.bc.err.item())
+        if e:
+            raise RuntimeError(f"beam device error word 0x{e:x} in member {self.name}")
+        return out
+
+    def release(self):
+        self.solver = None
+        self.bc = None
+        self.source = None
+        self.marks.clear()
+
+
+def make_member(config: dict, driver, device=None, name=None) -> Member:
+    """A Member for a rigid Gaussian driver, a BeamMember for a beam."""
+    if isinstance(driver, BeamDriver):
+        return BeamMember(config, driver, device, name)
+    return Member(config, driver, device, name)
+
+
+def solo_ez(config: dict, driver, **overrides) -> np.ndarray:
+    """On-axis Ez of the same simulation run alone through the drop-in
+    Simulation API (one time step), with config keys overridden."""
+    import os
+    import tempfile
+    from .simulation import Simulation
+    c = {**config, **overrides}
+    if isinstance(driver, BeamDriver):
+        c['rigid-beam'] = False
+        c.setdefault('time-limit', 1.0)
+        c['time-step'] = c.get('time-step', 1.0)
+        sim = Simulation(config=c, runas_filename='')
+        arr = driver.particles(float(c['xi-step']))
+        with tempfile.TemporaryDirectory() as d:
+            path = os.path.join(d, 'beam.npz')
+            np.savez(path, **{k: arr[k] for k in arr.dtype.names})
+            sim.load_beamfile(path)
+        sim.step(1)
+    else:
+        sim = Simulation(config=c, beam_parameters=driver, runas_filename='')
+        sim.step()
+    return sim.push_solver.ez_axis.cpu().numpy()
 
 
 class BatchRunner:
@@ -191,12 +352,15 @@ class BatchRunner:
 
 
 def request_stream(n=500, rate=20.0, seed=4321, dxi=0.05, h=0.05, sizes=(129, 257, 513),
-                   min_steps=200, max_steps=2000, precision="mixed"):
+                   min_steps=200, max_steps=2000, precision="mixed", beam_fraction=0.5,
+                   beam_particles=(100_000, 1_000_000)):
     """The served stream: n requests with Poisson arrivals of the given mean
     rate (exponential gaps), grid drawn from sizes, xi length uniform in
-    [min_steps, max_steps] steps of dxi, and a rigid Gaussian driver with
-    amplitude ~ U[0.01, 0.5] and sigma_r ~ U[0.5, 2]; all drawn from
-    numpy.random.default_rng(seed).  Returns (arrival, id, config, driver)."""
+    [min_steps, max_steps] steps of dxi, and a driver with amplitude ~
+    U[0.01, 0.5] and sigma_r ~ U[0.5, 2]: with probability beam_fraction a
+    non-rigid bi-Gaussian beam of U[beam_particles] macroparticles, else a
+    rigid Gaussian; all drawn from numpy.random.default_rng(seed).  Returns
+    (arrival, id, config, driver)."""
     widths = {129: 3.25, 257: 6.45, 513: 12.85}
     rng = np.random.default_rng(seed)
     t = 0.0
@@ -205,13 +369,20 @@ def request_stream(n=500, rate=20.0, seed=4321, dxi=0.05, h=0.05, sizes=(129, 25
         t += float(rng.exponential(1.0 / rate))
         N = int(sizes[rng.integers(len(sizes))])
         steps = int(rng.integers(min_steps, max_steps + 1))
-        drv = GaussianDriver(amplitude=float(rng.uniform(0.01, 0.5)),
-                             sigma_r=float(rng.uniform(0.5, 2.0)))
-        cfg = {'geometry': '3d', 'window-width': widths.get(N, N * h / 2), 'transverse-step': h,
+        amp, sig = float(rng.uniform(0.01, 0.5)), float(rng.uniform(0.5, 2.0))
+        width = widths.get(N, N * h / 2)
+        if rng.random() < beam_fraction:
+            # radial cut at 4 sigma_r, or at 80% of the window's half width
+            drv = BeamDriver(n=int(rng.integers(beam_particles[0], beam_particles[1] + 1)),
+                             amplitude=amp, sigma_r=sig, seed=seed * 1000 + r,
+                             r_max=min(4 * sig, 0.4 * width))
+        else:
+            drv = GaussianDriver(amplitude=amp, sigma_r=sig)
+        cfg = {'geometry': '3d', 'window-width': width, 'transverse-step': h,
                'window-length': (steps - 1) * dxi, 'xi-step': dxi,
                'ion-model': 'background', 'plasma-particles-per-cell': 4,
-               'rigid-beam': True, 'print-every': 0, 'precision': precision,
-               'time-step': 1.0}
+               'rigid-beam': not isinstance(drv, BeamDriver), 'print-every': 0,
+               'precision': precision, 'time-step': 1.0}
         out.append((t, f"req{r:04d}", cfg, drv))
     return out
 
@@ -280,11 +451,11 @@ class Server:
             arr, rid, cfg, drv = self.waiting[0]
             if arr > t or len(self.running) + len(self.draining) >= self.max_slots:
                 break
-            fp = footprint_bytes(cfg)
+            fp = footprint_bytes(cfg, drv)
             if self.used + fp > self.budget and (self.running or self.draining):
                 break
             self.waiting.popleft()
-            m = Member(cfg, drv, self.device, name=rid)
+            m = make_member(cfg, drv, self.device, name=rid)
             m.t_arrival = arr
             m.t_admit = t
             m.footprint = fp

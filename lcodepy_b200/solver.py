@@ -109,6 +109,10 @@ class Plane2d3vPlasmaSolver:
         self.graph_launches = [0, 0]
         self.graph_div = None
         self.eager_steps = 0
+        # capture on the current (non-default) stream without the device-wide
+        # synchronisation of torch.cuda.graph, for solvers that share the GPU
+        # with others (batch members)
+        self.capture_on_stream = False
 
     def _timed(self, name, fn, *args):
         if self.op_timers is None:
@@ -269,8 +273,15 @@ class Plane2d3vPlasmaSolver:
                 return
             g = torch.cuda.CUDAGraph()
             n0 = _lib.load().lcb_launch_count()
-            with torch.cuda.graph(g):
-                self._step_ops(self.rbf, self.rbp, rb_div, advance=False)
+            if self.capture_on_stream:
+                g.capture_begin(capture_error_mode="thread_local")
+                try:
+                    self._step_ops(self.rbf, self.rbp, rb_div, advance=False)
+                finally:
+                    g.capture_end()
+            else:
+                with torch.cuda.graph(g):
+                    self._step_ops(self.rbf, self.rbp, rb_div, advance=False)
             self.graph_launches[p] = _lib.load().lcb_launch_count() - n0
             self.graphs[p] = g
         self.graphs[p].replay()

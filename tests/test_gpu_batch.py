@@ -10,7 +10,8 @@ if not torch.cuda.is_available():  # pragma: no cover
     pytest.skip("needs CUDA", allow_module_level=True)
 
 from lcodepy_b200 import Simulation  # noqa: E402
-from lcodepy_b200.batch import BatchRunner, GaussianDriver, Member, Server  # noqa: E402
+from lcodepy_b200.batch import (BatchRunner, BeamDriver, BeamMember, GaussianDriver,  # noqa: E402
+                                Member, Server, solo_ez)
 
 
 def cfg(ww, n_steps, precision="fp64", dxi=0.05):
@@ -43,13 +44,31 @@ def test_batched_members_equal_solo_runs():
         assert rel(got, ref) < 1e-9
 
 
+def _beam(seed, amplitude=0.2):
+    # a short narrow electron driver that stays inside the 1.6-wide window
+    return BeamDriver(n=20_000, amplitude=amplitude, sigma_r=0.15, sigma_z=0.3, xi0=-0.5,
+                      seed=seed, r_max=0.5)
+
+
+def test_beam_member_equals_solo_run():
+    """A non-rigid driver in the batch engine (device beam layer step between
+    captured plasma steps) gives the drop-in Simulation's on-axis Ez."""
+    c, d = cfg(1.6, 30), _beam(3)
+    m = BeamMember(c, d)
+    BatchRunner([m]).run()
+    ref = solo_ez(c, d)
+    assert rel(m.result()["ez"], ref) < 1e-9
+    assert np.abs(ref).max() > 0
+
+
 def test_server_results_same_alone_and_in_the_mix():
     """Requests of different sizes and lengths admitted while others run, under
     a memory budget that forces some to wait: each result equals its solo run."""
     specs = {"a": (cfg(1.6, 40), GaussianDriver(0.2, 1.0)),
              "b": (cfg(3.25, 20), GaussianDriver(0.4, 0.7)),
              "c": (cfg(1.6, 15), GaussianDriver(0.1, 1.2)),
-             "d": (cfg(3.25, 35), GaussianDriver(0.3, 1.8))}
+             "d": (cfg(3.25, 35), GaussianDriver(0.3, 1.8)),
+             "e": (cfg(1.6, 25), _beam(7, 0.3))}
     from lcodepy_b200.batch import footprint_bytes
     budget = footprint_bytes(specs["b"][0]) + footprint_bytes(specs["a"][0]) + (1 << 20)
     srv = Server(hbm_budget_bytes=budget, max_slots=2)
@@ -61,4 +80,4 @@ def test_server_results_same_alone_and_in_the_mix():
     d = srv.done
     assert any(d[x]["admitted"] >= d[y]["finished"] for x in d for y in d if x != y)
     for rid, (c, d) in specs.items():
-        assert rel(srv.done[rid]["ez"], solo(c, d)) < 1e-9, rid
+        assert rel(srv.done[rid]["ez"], solo_ez(c, d)) < 1e-9, rid

@@ -33,7 +33,7 @@ class FakeMember:
 @pytest.fixture
 def fake(monkeypatch):
     monkeypatch.setattr(batch, "Member", FakeMember)
-    monkeypatch.setattr(batch, "footprint_bytes", lambda cfg: cfg["bytes"])
+    monkeypatch.setattr(batch, "footprint_bytes", lambda cfg, drv=None: cfg["bytes"])
 
 
 def req(steps, nbytes, cells=1):
@@ -91,3 +91,28 @@ def test_request_stream_is_seeded():
            [(r[0], r[2]['window-length'], r[3]) for r in b]
     arr = [r[0] for r in a]
     assert arr == sorted(arr) and arr[0] > 0
+
+
+def test_beam_driver_routes_to_beam_member_and_costs_more(monkeypatch):
+    made = []
+    monkeypatch.setattr(batch, "BeamMember", lambda *a: made.append(("beam", a[1])) or a)
+    monkeypatch.setattr(batch, "Member", lambda *a: made.append(("rigid", a[1])) or a)
+    drv = batch.BeamDriver(n=1000, amplitude=0.1, sigma_r=0.5)
+    batch.make_member({}, drv)
+    batch.make_member({}, batch.GaussianDriver(0.1, 1.0))
+    assert [k for k, _ in made] == ["beam", "rigid"]
+    cfg = {"geometry": "3d", "window-width-step-size": 0.05, "window-width": 6.4,
+           "xi-step": 0.05, "window-length": 1.0}
+    rigid = batch.footprint_bytes(cfg)
+    assert batch.footprint_bytes(cfg, drv) == rigid + 1000 * batch.BEAM_BYTES_PER_PARTICLE
+
+
+def test_request_stream_mixes_rigid_and_beam_drivers():
+    reqs = list(batch.request_stream(200, rate=20.0, seed=5))
+    kinds = {type(r[3]).__name__ for r in reqs}
+    assert kinds == {"BeamDriver", "GaussianDriver"}
+    for _, _, cfg, drv in reqs:
+        if isinstance(drv, batch.BeamDriver):
+            assert 100_000 <= drv.n <= 1_000_000
+            half = cfg["window-width"] / 2
+            assert drv.r_max < half
