@@ -424,22 +424,51 @@ __device__ __forceinline__ void weights4f(float x, float w[5])
 __device__ __forceinline__ void weights_of(float x, float w[5]) { weights4f(x, w); }
 __device__ __forceinline__ void weights_of(double x, double w[5]) { weights4(x, w); }
 
-// Row stride (in elements) of the field window: the two half-warps of a warp
-// work one cell apart along x, and a row stride of 16 (mod 32) words puts
-// their loads on disjoint banks (FP32: 16 mod 32 elements; FP64: 8 mod 16).
-template <int WY, typename FT>
-struct FieldStride {
-    static constexpr int v = sizeof(FT) == 4 ? ((WY + 15) / 32) * 32 + 16 : ((WY + 7) / 16) * 16 + 8;
+// Field window in shared memory: the six field values of a cell are stored
+// together, so that one stencil point of the gather takes vector loads
+// (FP32: a float4 of Ex, Ey, Ez, Bx and a float2 of By, Bz; FP64: three
+// double2) instead of six scalar ones.  A quarter warp reads eight
+// consecutive cells of a row (128 contiguous bytes per load), so rows need
+// no padding.
+template <typename FT> struct FieldWin;
+template <> struct FieldWin<float> {
+    static constexpr int bytes_per_cell = 24;
+    __device__ static void put(unsigned char *w, int ncell, int c, const float v[6])
+    {
+        reinterpret_cast<float4 *>(w)[c] = make_float4(v[0], v[1], v[2], v[3]);
+        reinterpret_cast<float2 *>(w + 16 * ncell)[c] = make_float2(v[4], v[5]);
+    }
+    __device__ static void get(const unsigned char *w, int ncell, int c, float v[6])
+    {
+        const float4 a = reinterpret_cast<const float4 *>(w)[c];
+        const float2 b = reinterpret_cast<const float2 *>(w + 16 * ncell)[c];
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y;
+    }
+};
+template <> struct FieldWin<double> {
+    static constexpr int bytes_per_cell = 48;
+    __device__ static void put(unsigned char *w, int ncell, int c, const double v[6])
+    {
+        double2 *d = reinterpret_cast<double2 *>(w);
+        d[c] = make_double2(v[0], v[1]);
+        d[ncell + c] = make_double2(v[2], v[3]);
+        d[2 * ncell + c] = make_double2(v[4], v[5]);
+    }
+    __device__ static void get(const unsigned char *w, int ncell, int c, double v[6])
+    {
+        const double2 *d = reinterpret_cast<const double2 *>(w);
+        const double2 a = d[c], b = d[ncell + c], e = d[2 * ncell + c];
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y; v[4] = e.x; v[5] = e.y;
+    }
 };
 
 // Midpoint gather of one particle from the window when the stencil fits in
 // it, else from the FP64 planes in HBM; weights and sums in FT.
 template <typename FT, int WX, int WY>
-__device__ __forceinline__ void gather_one(const FT *sf, const double *const *fld, int N,
+__device__ __forceinline__ void gather_one(const unsigned char *sf, const double *const *fld, int N,
                                            int wx0, int wy0, int ix, int iy, FT xl, FT yl,
                                            FT F[6])
 {
-    constexpr int FS = FieldStride<WY, FT>::v, FSZ = WX * FS;
     FT wx[5], wy[5];
     weights_of(xl, wx);
     weights_of(yl, wy);
@@ -450,9 +479,10 @@ __device__ __forceinline__ void gather_one(const FT *sf, const double *const *fl
 #pragma unroll
             for (int b = 0; b < 5; b++) {
                 const FT w = wx[a] * wy[b];
-                const int c = (lx + a) * FS + ly + b;
+                FT v[6];
+                FieldWin<FT>::get(sf, WX * WY, (lx + a) * WY + ly + b, v);
 #pragma unroll
-                for (int f = 0; f < 6; f++) F[f] += sf[f * FSZ + c] * w;
+                for (int f = 0; f < 6; f++) F[f] += v[f] * w;
             }
         }
     } else {
@@ -479,11 +509,15 @@ __device__ __forceinline__ void gather_one(const FT *sf, const double *const *fl
 // global 64-bit path instead), the high word below 2^30.
 constexpr double FIX_SHARED_LIMIT = 4398046511104.0;   // 2^42, on values scaled by 2^32 / h^2
 
-__device__ __forceinline__ void shared_fix_add(unsigned *lo, int *hi, int idx, fix_t c)
+// t = FIX_MAGIC + c exactly (the rounding FMA's result).  FIX_MAGIC's low
+// word is zero, so the low word of t's bit pattern is c mod 2^32 and its high
+// word minus 0x43380000 is floor(c / 2^32); c >> 20 is then one funnel shift.
+__device__ __forceinline__ void shared_fix_add(unsigned *lo, int *hi, int idx, double t)
 {
-    atomicAdd(lo + idx, (unsigned)c & 0xFFFFFu);
-    const int h = (int)((long long)c >> 20);
-    if (h) atomicAdd(hi + idx, h);
+    const unsigned w0 = (unsigned)__double2loint(t);
+    const unsigned w1 = (unsigned)(__double2hiint(t) - 0x43380000);
+    atomicAdd(lo + idx, w0 & 0xFFFFFu);
+    atomicAdd(hi + idx, (int)__funnelshift_r(w0, w1, 20));
 }
 
 __device__ __forceinline__ bool shared_fix_ok(const double sv[4])
@@ -511,7 +545,7 @@ __device__ __forceinline__ void deposit_fix_one(unsigned *swl, int *swh, fix_t *
                 const int c = (lx + a) * WY + ly + b;
 #pragma unroll
                 for (int q = 0; q < 4; q++)
-                    shared_fix_add(swl, swh, q * WSZ + c, fix_bits(fma(sv[q], w, FIX_MAGIC)));
+                    shared_fix_add(swl, swh, q * WSZ + c, fma(sv[q], w, FIX_MAGIC));
             }
         }
     } else {
@@ -558,12 +592,11 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
     typedef typename StageAcc<FT>::type Acc;
     static_assert(DEP_PPT == 2, "a thread owns two particles");
     constexpr int WSZ = WX * WY;
-    constexpr int FS = FieldStride<WY, FT>::v, FSZ = WX * FS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Acc *sw = reinterpret_cast<Acc *>(smem_raw);               // [4][WX][WY] deposit
     unsigned *swl = reinterpret_cast<unsigned *>(sw);          //   mixed: [4][WX][WY] low words
     int *swh = reinterpret_cast<int *>(swl + 4 * WSZ);         //   and [4][WX][WY] high words
-    FT *sf = reinterpret_cast<FT *>(sw + 4 * WSZ);             // [6][WX][FS] fields
+    unsigned char *sf = reinterpret_cast<unsigned char *>(sw + 4 * WSZ);  // fields, FieldWin
     const int s = blockIdx.z;
     const int64_t base = (int64_t)s * n_per_sort;
     const int half_n = N / 2;
@@ -597,9 +630,10 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
         const int gx = wx0 + t / WY, gy = wy0 + t % WY;
         const bool in = gx >= 0 && gx < N && gy >= 0 && gy < N;
         const int64_t g = (int64_t)gx * N + gy;
-        const int c = (t / WY) * FS + t % WY;
+        FT v[6];
 #pragma unroll
-        for (int f = 0; f < 6; f++) sf[f * FSZ + c] = in ? (FT)__ldg(fld[f] + g) : FT(0);
+        for (int f = 0; f < 6; f++) v[f] = in ? (FT)__ldg(fld[f] + g) : FT(0);
+        FieldWin<FT>::put(sf, WSZ, t, v);
     }
     __syncthreads();
 
@@ -676,12 +710,12 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
 #pragma unroll
                 for (int b = 0; b < 5; b++) {
                     const FT wa = ax[a] * ay[b], wb = bx[a] * by[b];
-                    const int c = (lx + a) * FS + ly + b;
+                    FT v[6];
+                    FieldWin<FT>::get(sf, WSZ, (lx + a) * WY + ly + b, v);
 #pragma unroll
                     for (int f = 0; f < 6; f++) {
-                        const FT v = sf[f * FSZ + c];
-                        F0[f] += v * wa;
-                        F1[f] += v * wb;
+                        F0[f] += v[f] * wa;
+                        F1[f] += v[f] * wb;
                     }
                 }
             }
@@ -710,22 +744,27 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
         const double xi0 = x_init[k], yi0 = y_init[k];
         double px = opx, py = opy, pz = opz;
         if (zero_p[p]) px = py = pz = 0;
-        double gm = sqrt(mk * mk + px * px + py * py + pz * pz);
-        double ig = 1.0 / gm;
-        double vx = px * ig, vy = py * ig, vz = pz * ig;
-        double f = qk * xi_step / (1 - vz);
-        double dpx = f * (Ex + vy * Bz - vz * By);
-        double dpy = f * (Ey - vx * Bz + vz * Bx);
-        double dpz = f * (Ez + vx * By - vy * Bx);
-        px = opx + dpx * 0.5; py = opy + dpy * 0.5; pz = opz + dpz * 0.5;
-        gm = sqrt(mk * mk + px * px + py * py + pz * pz);
-        ig = 1.0 / gm;
-        vx = px * ig; vy = py * ig; vz = pz * ig;
-        f = qk * xi_step / (1 - vz);
-        dpx = f * (Ex + vy * Bz - vz * By);
-        dpy = f * (Ey - vx * Bz + vz * Bx);
-        dpz = f * (Ez + vx * By - vy * Bx);
-        px = opx + dpx * 0.5; py = opy + dpy * 0.5; pz = opz + dpz * 0.5;
+        double gm, dpx, dpy, dpz;
+#pragma unroll
+        for (int it = 0; it < 2; it++) {
+            gm = sqrt(mk * mk + px * px + py * py + pz * pz);
+            if (MIXED) {
+                // f (E + v x B) with v = p / gm and f = q dxi / (1 - vz),
+                // as q dxi (gm E + p x B) / (gm - pz): one quotient
+                const double r = qk * xi_step / (gm - pz);
+                dpx = r * (gm * Ex + py * Bz - pz * By);
+                dpy = r * (gm * Ey - px * Bz + pz * Bx);
+                dpz = r * (gm * Ez + px * By - py * Bx);
+            } else {
+                const double ig = 1.0 / gm;
+                const double vx = px * ig, vy = py * ig, vz = pz * ig;
+                const double f = qk * xi_step / (1 - vz);
+                dpx = f * (Ex + vy * Bz - vz * By);
+                dpy = f * (Ey - vx * Bz + vz * Bx);
+                dpz = f * (Ez + vx * By - vy * Bx);
+            }
+            px = opx + dpx * 0.5; py = opy + dpy * 0.5; pz = opz + dpz * 0.5;
+        }
         gm = sqrt(mk * mk + px * px + py * py + pz * pz);
         const double adv = xi_step / (gm - pz);
         double xo = xo_p[k] + px * adv;
@@ -746,10 +785,17 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
         if (FIRST || absorbed) q_f[k] = absorbed ? 0.0 : qk;
         if (absorbed) continue;
         const double gd = sqrt(mk * mk + px * px + py * py + pz * pz);
-        const double igd = 1.0 / gd;
-        const double dro = qk / (1 - pz * igd);
-        const double rg = dro * igd;
-        const double djx = px * rg, djy = py * rg, djz = pz * rg;
+        double dro, djx, djy, djz;
+        if (MIXED) {
+            // q / (1 - pz / gd) and p q / (gd - pz): one quotient
+            const double r = qk / (gd - pz);
+            dro = r * gd; djx = r * px; djy = r * py; djz = r * pz;
+        } else {
+            const double igd = 1.0 / gd;
+            dro = qk / (1 - pz * igd);
+            const double rg = dro * igd;
+            djx = px * rg; djy = py * rg; djz = pz * rg;
+        }
         if (MIXED) check_range<fix_t>(dro, djx, djy, djz, ih, err);
         const int c_x = cell_of((MIXED ? (xi0 + xo) * ih : (xi0 + xo) / h) + 0.5, half_n, dxl[p]);
         const int c_y = cell_of((MIXED ? (yi0 + yo) * ih : (yi0 + yo) / h) + 0.5, half_n, dyl[p]);
@@ -784,7 +830,7 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
 #pragma unroll
                         for (int q = 0; q < 4; q++)
                             shared_fix_add(swl, swh, q * WSZ + c,
-                                           fix_bits(fma(sv[0][q], wa, fma(sv[1][q], wb, FIX_MAGIC))));
+                                           fma(sv[0][q], wa, fma(sv[1][q], wb, FIX_MAGIC)));
                     }
                 }
             } else {
@@ -846,8 +892,8 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
 template <typename FT, int WX, int WY>
 static size_t move_deposit_pair_smem()
 {
-    return (size_t)WX * (FieldStride<WY, FT>::v * 6 * sizeof(FT) +
-                         WY * 4 * sizeof(typename StageAcc<FT>::type));
+    return (size_t)WX * WY * (FieldWin<FT>::bytes_per_cell +
+                              4 * sizeof(typename StageAcc<FT>::type));
 }
 
 template <typename FT, int WX, int WY, bool FIRST>
