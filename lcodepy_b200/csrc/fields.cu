@@ -501,6 +501,21 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
     const unsigned tmem = *tslot;
     const unsigned idesc = i8_idesc<BN>();
 
+    // epilogue layout: warp w stores TMEM lanes 32 (w % 4) .. + 31 (tile rows)
+    // and columns CW (w / 4) .. + CW - 1; pass `it` of a lane covers element
+    // it * 32 + lane of the warp's 32 x CW block (lanes along a row).  The
+    // values the epilogue reads (spectral factors, previous fields) are
+    // loaded here, so that their latency hides behind the main loop.
+    constexpr int CW = BN / 2;            // columns per warp
+    const int rq = warp & 3, ch = warp >> 2;
+    double pre[CW];
+#pragma unroll
+    for (int it = 0; it < CW; it++) {
+        const int e = it * 32 + lane, row = e / CW, col = e % CW;
+        const int gm = m0 + 32 * rq + row, gn = n0 + CW * ch + col;
+        pre[it] = (EPI != EPI_STORE && gm < M && gn < N) ? epi_pre<EPI, T>(batch, g, gm, gn) : 0.0;
+    }
+
     bool ok = true;
     if (warp == 0) {
         // warp 0 streams the stages (eight bulk copies each: four A and four
@@ -565,14 +580,10 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
     ok &= mbar_wait(smem_u32(fin), 0);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
-    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (tile rows) and
-    // columns 32 (w / 4) .. + 31; the NS accumulators combine exactly in
-    // 64-bit integers, four at a time (a0 2^21 + a1 2^14 + a2 2^7 + a3,
-    // |.| < 2^53), with one conversion per four; the values go through shared
-    // memory (the pipeline buffers are free now) so that the stores run along
-    // rows
-    constexpr int CW = BN / 2;            // columns per warp
-    const int rq = warp & 3, ch = warp >> 2;
+    // epilogue: the NS accumulators combine exactly in 64-bit integers, four
+    // at a time (a0 2^21 + a1 2^14 + a2 2^7 + a3, |.| < 2^53), with one
+    // conversion per four; the values go through shared memory (the pipeline
+    // buffers are free now) so that the stores run along rows
     T *stage = reinterpret_cast<T *>(i8sm) + warp * 32 * (CW + 1);
     const double scale = ldexp(1.0, ea + eb - 33);
 #pragma unroll 1
@@ -606,25 +617,12 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
     __syncwarp();
     double part = 0;
     float vmax = 0.f;
-    // the warp's 32 x CW values, 32 per pass with lanes along a row; passes
-    // in groups of 8, whose scale factors or previous fields are loaded
-    // before any store
-#pragma unroll 1
-    for (int it0 = 0; it0 < CW; it0 += 8) {
-        double pre[8];
 #pragma unroll
-        for (int u = 0; u < 8; u++) {
-            const int e = (it0 + u) * 32 + lane, row = e / CW, col = e % CW;
-            const int gm = m0 + 32 * rq + row, gn = n0 + CW * ch + col;
-            pre[u] = (gm < M && gn < N) ? epi_pre<EPI, T>(batch, g, gm, gn) : 0.0;
-        }
-#pragma unroll
-        for (int u = 0; u < 8; u++) {
-            const int e = (it0 + u) * 32 + lane, row = e / CW, col = e % CW;
-            const int gm = m0 + 32 * rq + row, gn = n0 + CW * ch + col;
-            if (gm >= M || gn >= N) continue;
-            part += epi_apply<EPI, T>(batch, g, gm, gn, stage[row * (CW + 1) + col], pre[u], vmax);
-        }
+    for (int it = 0; it < CW; it++) {
+        const int e = it * 32 + lane, row = e / CW, col = e % CW;
+        const int gm = m0 + 32 * rq + row, gn = n0 + CW * ch + col;
+        if (gm >= M || gn >= N) continue;
+        part += epi_apply<EPI, T>(batch, g, gm, gn, stage[row * (CW + 1) + col], pre[it], vmax);
     }
     if (EPI != EPI_FIELD && batch.amax_out) {
 #pragma unroll
@@ -686,68 +684,71 @@ __device__ __forceinline__ void put_slices4(uint8_t *blk, int64_t plane, int64_t
     for (int i = 0; i < NS; i++) *reinterpret_cast<unsigned *>(blk + i * plane + at) = w[i];
 }
 
-// Block: 32 x 4 threads, four output rows (threadIdx.y) with 32 threads
-// striding over each row's groups of four.
+// One thread per 32-bit word of every slice plane (four consecutive
+// elements): a warp covers a core matrix's eight rows (lanes 0-7) by four
+// groups of four elements (lanes / 8), so that each of its stores writes
+// 128 contiguous bytes per plane; the source elements are read straight from
+// L2.  Column folds (A role, feeding right waves) pair element j with
+// C - 1 - j of the same row; row folds (B role, feeding left waves) pair rows
+// k and R - 1 - k.
+constexpr int FOLD_THREADS = 256;
+
 template <typename T>
-__global__ void __launch_bounds__(128) k_fold_slices(const __grid_constant__ FoldBatch<T> fb)
+__global__ void __launch_bounds__(FOLD_THREADS) k_fold_slices(const __grid_constant__ FoldBatch<T> fb)
 {
     constexpr int NS = Slices<T>::n;
     const FoldDesc<T> &f = fb.d[blockIdx.z];
     const int R = f.R, C = f.C, ldc = ld2(C);
-    if (fb.clear && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.y == 0 &&
-        threadIdx.x < NPROB)
+    if (fb.clear && blockIdx.x == 0 && blockIdx.z == 0 && threadIdx.x < NPROB)
         fb.clear[threadIdx.x] = 0u;
-    const int row0 = blockIdx.y * blockDim.y + threadIdx.y, rstep = gridDim.y * blockDim.y;
-    const double scale = ldexp(1.0, -bound_exp(2.f * __uint_as_float(*f.src_max)));
+    const int idx = blockIdx.x * FOLD_THREADS + threadIdx.x, lane = idx & 31, w = idx >> 5;
     uint8_t *blk = reinterpret_cast<uint8_t *>(f.dst);
     if (!f.by_rows) {
         const int he = (C + 1) / 2, ho = C - he, mid = (C - 1) / 2;
-        const int Rp = ntiles(R, TL_M) * TL_M;
         const int KTu = ntiles(he, TL_K), KTv = ntiles(ho, TL_K);
-        const int64_t pu = a_plane_bytes(R, he), pv = a_plane_bytes(R, ho);
-        for (int y = row0; y < 2 * Rp; y += rstep) {
-            const bool isv = y >= Rp;
-            const int r = isv ? y - Rp : y;
-            const int KT = isv ? KTv : KTu, groups = KT * TL_K / 4;
-            const T *row = f.src + (int64_t)(r < R ? r : 0) * ldc;
-            for (int t = threadIdx.x; t < groups; t += blockDim.x) {
-                T v[4];
+        const int nu = 2 * KTu, nkb = nu + 2 * KTv;     // 16-wide k blocks of U, then of V
+        const int rb = w / nkb, kb = w - rb * nkb;
+        const int r = rb * 8 + (lane & 7);
+        if (r >= ntiles(R, TL_M) * TL_M) return;
+        const double scale = ldexp(1.0, -bound_exp(2.f * __uint_as_float(*f.src_max)));
+        const bool isv = kb >= nu;
+        const int k = (isv ? kb - nu : kb) * 16 + (lane >> 3) * 4;
+        const T *x = f.src + (int64_t)(r < R ? r : 0) * ldc;
+        T v[4];
 #pragma unroll
-                for (int e = 0; e < 4; e++) {
-                    const int j = 4 * t + e;
-                    if (r >= R) v[e] = T(0);
-                    else if (!isv) v[e] = j < mid ? row[j] + row[C - 1 - j] : (j == mid ? row[mid] : T(0));
-                    else v[e] = j < ho ? row[j] - row[C - 1 - j] : T(0);
-                }
-                if (!isv) put_slices4<NS>(blk, pu, a_tile_off(r, 4 * t, KTu), v, scale);
-                else put_slices4<NS>(blk + NS * pu, pv, a_tile_off(r, 4 * t, KTv), v, scale);
-            }
+        for (int e = 0; e < 4; e++) {
+            const int j = k + e;
+            if (r >= R) v[e] = T(0);
+            else if (!isv) v[e] = j < mid ? x[j] + x[C - 1 - j] : (j == mid ? x[mid] : T(0));
+            else v[e] = j < ho ? x[j] - x[C - 1 - j] : T(0);
         }
+        if (!isv) put_slices4<NS>(blk, a_plane_bytes(R, he), a_tile_off(r, k, KTu), v, scale);
+        else put_slices4<NS>(blk + NS * a_plane_bytes(R, he), a_plane_bytes(R, ho),
+                             a_tile_off(r, k, KTv), v, scale);
     } else {
         const int he = (R + 1) / 2, ho = R - he, mid = (R - 1) / 2;
         const int KTu = ntiles(he, TL_K), KTv = ntiles(ho, TL_K);
-        const int Kpu = KTu * TL_K, Kpv = KTv * TL_K;
-        const int groups = ntiles(C, TL_N) * TL_N / 4;
-        const int64_t pu = b_plane_bytes(he, C), pv = b_plane_bytes(ho, C);
-        for (int y = row0; y < Kpu + Kpv; y += rstep) {
-            const bool isv = y >= Kpu;
-            const int k = isv ? y - Kpu : y;
-            const bool valid = isv ? k < ho : k < he;
-            const T *ra = f.src + (int64_t)(valid ? k : 0) * ldc;
-            const T *rb = f.src + (int64_t)(valid ? R - 1 - k : 0) * ldc;
-            const bool single = !isv && k == mid;
-            for (int t = threadIdx.x; t < groups; t += blockDim.x) {
-                T v[4];
+        const int ng = ntiles(C, TL_N) * 4, ntask = 2 * ng;  // 16-wide n groups of U, then of V
+        const int kb = w / ntask, t = w - kb * ntask;
+        const int k = kb * 8 + (lane & 7);
+        if (k >= KTu * TL_K) return;
+        const bool isv = t >= ng;
+        if (isv && k >= KTv * TL_K) return;
+        const double scale = ldexp(1.0, -bound_exp(2.f * __uint_as_float(*f.src_max)));
+        const int n = (isv ? t - ng : t) * 16 + (lane >> 3) * 4;
+        const bool valid = isv ? k < ho : k < he;
+        const T *ra = f.src + (int64_t)(valid ? k : 0) * ldc;
+        const T *rb = f.src + (int64_t)(valid ? R - 1 - k : 0) * ldc;
+        const bool single = !isv && k == mid;
+        T v[4];
 #pragma unroll
-                for (int e = 0; e < 4; e++) {
-                    const int n = 4 * t + e;
-                    v[e] = (!valid || n >= C) ? T(0)
-                         : (single ? ra[n] : (isv ? ra[n] - rb[n] : ra[n] + rb[n]));
-                }
-                if (!isv) put_slices4<NS>(blk, pu, b_tile_off(k, 4 * t, KTu), v, scale);
-                else put_slices4<NS>(blk + NS * pu, pv, b_tile_off(k, 4 * t, KTv), v, scale);
-            }
+        for (int e = 0; e < 4; e++) {
+            const int c = n + e;
+            v[e] = (!valid || c >= C) ? T(0) : (single ? ra[c] : (isv ? ra[c] - rb[c] : ra[c] + rb[c]));
         }
+        if (!isv) put_slices4<NS>(blk, b_plane_bytes(he, C), b_tile_off(k, n, KTu), v, scale);
+        else put_slices4<NS>(blk + NS * b_plane_bytes(he, C), b_plane_bytes(ho, C),
+                             b_tile_off(k, n, KTv), v, scale);
     }
 }
 
@@ -1044,11 +1045,14 @@ static int run_fold(T *const *src, T *const *dst, const int *probs, int np, cons
         fb.d[q].src_max = src_max ? src_max + p : nullptr;
     }
     fb.clear = clear;
-    // output rows: 2 x 128-padded rows (column fold) or the two 32-padded
-    // halves (row fold), four per block
-    const int nrows = by_rows ? ntiles((N + 1) / 2, TL_K) * TL_K * 2 : 2 * ntiles(N, TL_M) * TL_M;
-    dim3 grid(1u, (unsigned)((nrows + 3) / 4), np);
-    k_fold_slices<T><<<grid, dim3(32, 4), 0, st>>>(fb);
+    // threads per problem: one per slice word of the largest problem (rows
+    // padded to 8, words of 4 elements)
+    const int he = (N + 1) / 2;
+    const int64_t words = by_rows
+        ? (int64_t)ntiles(he, TL_K) * TL_K * ntiles(N, TL_N) * TL_N * 2 / 4
+        : (int64_t)ntiles(N, TL_M) * TL_M * ntiles(he, TL_K) * TL_K * 2 / 4;
+    dim3 grid((unsigned)((words + FOLD_THREADS - 1) / FOLD_THREADS), 1u, np);
+    k_fold_slices<T><<<grid, FOLD_THREADS, 0, st>>>(fb);
     LCB_LAUNCH_CHECK("k_fold_slices");
     return LCB_OK;
 }
