@@ -608,23 +608,59 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
     // Tiles start on a lattice row whose cell also holds the next row, so
     // that a thread's two rows (ti, ti + 1 with ti even) share a cell: when
     // rows 0 and 1 sit in different cells the tiles are shifted up by one
-    // row (the grid has one spare row of tiles for it).
+    // row (the grid has one spare row of tiles for it).  The tile's first
+    // particle is read for both possible shifts at once, so that the tile
+    // origin costs one round trip to memory.
     double dummy;
-    int off = 0;
-    if (Ns > 1 && cell_of(x_init[base] / h + 0.5, half_n, dummy) !=
-                  cell_of(x_init[base + Ns] / h + 0.5, half_n, dummy))
-        off = 1;
+    const int ia = blockIdx.y * DEP_TI, ib = ia > 0 ? ia - 1 : 0;   // tile row for off = 0, 1
+    const int64_t ka = base + (int64_t)(ia < Ns ? ia : 0) * Ns + blockIdx.x * DEP_TJ;
+    const int64_t kb = base + (int64_t)ib * Ns + blockIdx.x * DEP_TJ;
+    const bool two_rows = Ns > 1;
+    const double r0x = x_init[base], r1x = two_rows ? x_init[base + Ns] : r0x;
+    const double xa = x_init[ka], ya = y_init[ka], xb = x_init[kb], yb = y_init[kb];
+    const double xa1 = ia + 1 < Ns ? x_init[ka + Ns] : xa, xb1 = ib + 1 < Ns ? x_init[kb + Ns] : xb;
+    const int off = (two_rows && cell_of(r0x / h + 0.5, half_n, dummy) !=
+                                 cell_of(r1x / h + 0.5, half_n, dummy)) ? 1 : 0;
     const int i0 = blockIdx.y * DEP_TI - off, j0 = blockIdx.x * DEP_TJ;
     const int ir = i0 < 0 ? 0 : i0;
     if (ir >= Ns) return;
     const int64_t k0 = base + (int64_t)ir * Ns + j0;
-    const int wx0 = cell_of(x_init[k0] / h + 0.5, half_n, dummy) - 2 - DEP_SLACK;
-    const int wy0 = cell_of(y_init[k0] / h + 0.5, half_n, dummy) - 2 - DEP_SLACK;
+    const double x0 = off ? xb : xa, y0 = off ? yb : ya, x1 = off ? xb1 : xa1;
+    const int wx0 = cell_of(x0 / h + 0.5, half_n, dummy) - 2 - DEP_SLACK;
+    const int wy0 = cell_of(y0 / h + 0.5, half_n, dummy) - 2 - DEP_SLACK;
     bool two = false;
     if (ir + 1 < Ns) {
-        const double d = x_init[k0 + Ns] - x_init[k0];
+        const double d = x1 - x0;
         two = fabs(2 * d - h) < 0.25 * h;
     }
+    (void)k0;
+
+    // ---- the particles' first loads, issued before the window fill ----
+    int64_t kk[2];
+    bool live[2], zero_p[2];
+    double L_xo0[2], L_yo0[2], L_xi[2], L_yi[2], L_q[2], L_xof[2], L_yof[2];
+    double L_m[2], L_px[2], L_py[2], L_pz[2];
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+        int ti, tj;
+        tile_slot(threadIdx.x + p * DEP_THREADS, two, ti, tj);
+        const int i = i0 + ti, j = j0 + tj;
+        live[p] = i >= 0 && i < Ns && j < Ns;
+        kk[p] = base + (int64_t)i * Ns + j;
+        L_xo0[p] = L_yo0[p] = L_xi[p] = L_yi[p] = L_q[p] = L_xof[p] = L_yof[p] = 0;
+        L_m[p] = L_px[p] = L_py[p] = L_pz[p] = 0;
+        if (!live[p]) continue;
+        const int64_t k = kk[p];
+        L_xo0[p] = xo_p[k]; L_yo0[p] = yo_p[k];
+        L_xi[p] = x_init[k]; L_yi[p] = y_init[k];
+        if (FIRST) {
+            L_m[p] = m_a[k]; L_px[p] = px_p[k]; L_py[p] = py_p[k]; L_pz[p] = pz_p[k];
+            L_q[p] = q_p[k];
+        } else {
+            L_q[p] = q_f[k]; L_xof[p] = xo_f[k]; L_yof[p] = yo_f[k];
+        }
+    }
+
     for (int t = threadIdx.x; t < 4 * WSZ; t += blockDim.x) sw[t] = Acc(0);
     for (int t = threadIdx.x; t < WSZ; t += blockDim.x) {
         const int gx = wx0 + t / WY, gy = wy0 + t % WY;
@@ -638,27 +674,20 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
     __syncthreads();
 
     // ---- phase 1: K1 (first stage) and the midpoint of each particle ----
-    int64_t kk[2];
-    bool live[2], zero_p[2];
     int ix[2], iy[2];
     FT xlf[2], ylf[2];
 #pragma unroll
     for (int p = 0; p < 2; p++) {
-        int ti, tj;
-        tile_slot(threadIdx.x + p * DEP_THREADS, two, ti, tj);
-        const int i = i0 + ti, j = j0 + tj;
-        live[p] = i >= 0 && i < Ns && j < Ns;
         zero_p[p] = false;
         ix[p] = iy[p] = -1000;
         xlf[p] = ylf[p] = FT(0);
-        kk[p] = base + (int64_t)i * Ns + j;
         if (!live[p]) continue;
         const int64_t k = kk[p];
-        const double xo0 = xo_p[k], yo0 = yo_p[k];
-        double qk, xof, yof;
+        const double xo0 = L_xo0[p], yo0 = L_yo0[p];
+        const double qk = L_q[p];
+        double xof, yof;
         if (FIRST) {
-            const double mk = m_a[k], opx = px_p[k], opy = py_p[k], opz = pz_p[k];
-            qk = q_p[k];
+            const double mk = L_m[p], opx = L_px[p], opy = L_py[p], opz = L_pz[p];
             xof = xo0; yof = yo0;
             if (mk != 0) {
                 const double gm = sqrt(mk * mk + opz * opz + opx * opx + opy * opy);
@@ -672,12 +701,11 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
                 q_f[k] = qk;
             }
         } else {
-            qk = q_f[k];
-            xof = xo_f[k]; yof = yo_f[k];
+            xof = L_xof[p]; yof = L_yof[p];
         }
         if (qk == 0) { live[p] = false; continue; }
-        double xh = x_init[k] + (xo0 + xof) / 2;
-        double yh = y_init[k] + (yo0 + yof) / 2;
+        double xh = L_xi[p] + (xo0 + xof) / 2;
+        double yh = L_yi[p] + (yo0 + yof) / 2;
         bool z = false;
         if (xh > boundary)  { xh =  2 * boundary - xh; z = true; }
         if (xh < -boundary) { xh = -2 * boundary - xh; z = true; }
@@ -693,6 +721,10 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
             if (err) atomicOr(err, LCB_DEVERR_PLASMA_STENCIL);
             ix[p] = -1000;  // no gather: zero fields, as in the reference's skip
         }
+        // FP64: the push's mass and momenta, loaded while the gather runs
+        // (in mixed precision the registers they would hold cost more spills
+        // than the early loads save)
+        if (!FIRST && !MIXED) { L_m[p] = m_a[k]; L_px[p] = px_p[k]; L_py[p] = py_p[k]; L_pz[p] = pz_p[k]; }
     }
 
     // ---- phase 2: gather ----
@@ -739,8 +771,9 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
         const int64_t k = kk[p];
         const FT *Fp = p ? F1 : F0;
         const double Ex = Fp[0], Ey = Fp[1], Ez = Fp[2], Bx = Fp[3], By = Fp[4], Bz = Fp[5];
-        const double mk = m_a[k], qk = FIRST ? q_p[k] : q_f[k];
-        const double opx = px_p[k], opy = py_p[k], opz = pz_p[k];
+        if (!FIRST && MIXED) { L_m[p] = m_a[k]; L_px[p] = px_p[k]; L_py[p] = py_p[k]; L_pz[p] = pz_p[k]; }
+        const double mk = L_m[p], qk = L_q[p];
+        const double opx = L_px[p], opy = L_py[p], opz = L_pz[p];
         const double xi0 = x_init[k], yi0 = y_init[k];
         double px = opx, py = opy, pz = opz;
         if (zero_p[p]) px = py = pz = 0;
