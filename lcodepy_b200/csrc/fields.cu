@@ -761,6 +761,7 @@ __global__ void __launch_bounds__(FOLD_THREADS) k_fold_slices(const __grid_const
 struct RhsArgs {
     int N;
     double h, dxi, c, rb_div;
+    double i2h, idxi, irb;                    // 1 / (2 h), 1 / dxi, 1 / rb_div
     const double *ro_f, *jx_f, *jy_f, *jz_f;  // full currents, n_f planes
     const double *ro_p, *jx_p, *jy_p, *jz_p;  // prev currents, n_p planes
     int n_f, n_p;
@@ -791,16 +792,15 @@ __device__ __forceinline__ void rhs_node(const RhsArgs &a, const double (*s_ro)[
     const int64_t plane = (int64_t)N * N;
     const int64_t t = (int64_t)i * N + j;
     const bool inner = i >= 1 && i < N - 1 && j >= 1 && j < N - 1;
-    const double h2 = a.h * 2;
     double dro_dx = 0, dro_dy = 0, djz_dx = 0, djz_dy = 0;
     if (inner) {
-        dro_dx = (s_ro[li + 1][lj] - s_ro[li - 1][lj]) / h2;
-        dro_dy = (s_ro[li][lj + 1] - s_ro[li][lj - 1]) / h2;
-        djz_dx = (s_jz[li + 1][lj] - s_jz[li - 1][lj]) / h2;
-        djz_dy = (s_jz[li][lj + 1] - s_jz[li][lj - 1]) / h2;
+        dro_dx = (s_ro[li + 1][lj] - s_ro[li - 1][lj]) * a.i2h;
+        dro_dy = (s_ro[li][lj + 1] - s_ro[li][lj - 1]) * a.i2h;
+        djz_dx = (s_jz[li + 1][lj] - s_jz[li - 1][lj]) * a.i2h;
+        djz_dy = (s_jz[li][lj + 1] - s_jz[li][lj - 1]) * a.i2h;
     }
-    const double djx_dxi = (psum(a.jx_p, a.n_p, plane, t) - s_jx[li][lj]) / a.dxi;
-    const double djy_dxi = (psum(a.jy_p, a.n_p, plane, t) - s_jy[li][lj]) / a.dxi;
+    const double djx_dxi = (psum(a.jx_p, a.n_p, plane, t) - s_jx[li][lj]) * a.idxi;
+    const double djy_dxi = (psum(a.jy_p, a.n_p, plane, t) - s_jy[li][lj]) * a.idxi;
     const double Ex_rhs = -(dro_dx - djx_dxi - a.c * a.Ex[t]);
     const double Ey_rhs = -(dro_dy - djy_dxi - a.c * a.Ey[t]);
     const double Bx_rhs = +(djz_dy - djy_dxi + a.c * a.Bx[t]);
@@ -820,14 +820,14 @@ __device__ __forceinline__ void rhs_node(const RhsArgs &a, const double (*s_ro)[
         djx_dy = s_jx[li][lj + 1] - s_jx[li][lj - 1];
         djy_dx = s_jy[li + 1][lj] - s_jy[li - 1][lj];
     }
-    const double bz_rhs = -(djx_dy - djy_dx) / h2;
+    const double bz_rhs = -(djx_dy - djy_dx) * a.i2h;
     X6[(int64_t)i * ldN + j] = (T)bz_rhs;
     mx[6] = fmaxf(mx[6], abs_bound((T)bz_rhs));
     if (inner) {
         const int64_t o = (int64_t)(i - 1) * ldn + (j - 1);
         const double djx_dx = s_jx[li + 1][lj] - s_jx[li - 1][lj];
         const double djy_dy = s_jy[li][lj + 1] - s_jy[li][lj - 1];
-        const double ez_rhs = -(djx_dx + djy_dy) / h2;
+        const double ez_rhs = -(djx_dx + djy_dy) * a.i2h;
         X4[o] = (T)ez_rhs;
         mx[4] = fmaxf(mx[4], abs_bound((T)ez_rhs));
         if (a.with_phi) {
@@ -857,7 +857,7 @@ k_fields_rhs(RhsArgs a, T *X0, T *X1, T *X2, T *X3, T *X4, T *X5, T *X6)
         double ro = 0, jz = 0, jx = 0, jy = 0;
         if (gi >= 0 && gi < N && gj >= 0 && gj < N) {
             const int64_t q = (int64_t)gi * N + gj;
-            const double rbf = a.rb_full[q] / a.rb_div, rbp = a.rb_prev[q] / a.rb_div;
+            const double rbf = a.rb_full[q] * a.irb, rbp = a.rb_prev[q] * a.irb;
             // (full + rho_beam_full + prev + rho_beam_prev) / 2, fields.py:194-197
             ro = (psum(a.ro_f, a.n_f, plane, q) + rbf + psum(a.ro_p, a.n_p, plane, q) + rbp) / 2;
             jz = (psum(a.jz_f, a.n_f, plane, q) + rbf + psum(a.jz_p, a.n_p, plane, q) + rbp) / 2;
@@ -1069,6 +1069,8 @@ static int solve(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st
     RhsArgs r;
     r.N = N; r.h = a->h; r.dxi = a->xi_step; r.c = a->subtraction_coeff;
     r.rb_div = a->rho_beam_divisor;
+    // the kernel multiplies by reciprocals (at most an ulp from the quotients)
+    r.i2h = 1.0 / (2.0 * a->h); r.idxi = 1.0 / a->xi_step; r.irb = 1.0 / a->rho_beam_divisor;
     r.ro_f = a->currents_full.ro; r.jx_f = a->currents_full.jx;
     r.jy_f = a->currents_full.jy; r.jz_f = a->currents_full.jz;
     r.n_f = a->currents_full.n_planes;
