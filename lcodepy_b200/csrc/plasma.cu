@@ -967,25 +967,43 @@ static int dispatch_move_deposit_pair(const lcb_move_deposit_args *a,
 }
 
 // Fixed-point sums (4 quantities x 2 columns x N*N) to the FP64 outputs;
-// columns past n_sorts get the background ions (ro) or zero.
+// columns past n_sorts get the background ions (ro) or zero.  A thread
+// takes one node of both columns.
 __global__ void k_fix_finish(int64_t plane, int n_sorts, const fix_t *__restrict__ w,
                              const double *__restrict__ ro_initial, double *ro, double *jx,
                              double *jy, double *jz)
 {
     double *outs[4] = {ro, jx, jy, jz};
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 2 * plane;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < plane;
          t += (int64_t)gridDim.x * blockDim.x) {
-        const int col = (int)(t / plane);
+        double v[8];
 #pragma unroll
         for (int qd = 0; qd < 4; qd++) {
-            double v;
-            if (col < n_sorts)
-                v = (double)(long long)w[qd * 2 * plane + t] * FIX_INV;
-            else
-                v = (qd == 0 && ro_initial) ? ro_initial[t - plane] : 0.0;
-            outs[qd][t] = v;
+            v[2 * qd] = (double)(long long)w[qd * 2 * plane + t] * FIX_INV;
+            v[2 * qd + 1] = n_sorts > 1 ? (double)(long long)w[qd * 2 * plane + plane + t] * FIX_INV
+                          : ((qd == 0 && ro_initial) ? ro_initial[t] : 0.0);
+        }
+#pragma unroll
+        for (int qd = 0; qd < 4; qd++) {
+            outs[qd][t] = v[2 * qd];
+            outs[qd][plane + t] = v[2 * qd + 1];
         }
     }
+}
+
+// Zero the columns of the fixed-point sums that the deposit adds to: all
+// eight planes with two sorts, else the first column of each quantity.
+static int clear_fixed(fix_t *w, size_t plane, int n_sorts, cudaStream_t st)
+{
+    if (n_sorts > 1) {
+        cudaError_t e = cudaMemsetAsync(w, 0, 8 * plane * sizeof(fix_t), st);
+        return e != cudaSuccess ? cuda_check(e, "memset fixed-point sums") : LCB_OK;
+    }
+    for (int qd = 0; qd < 4; qd++) {
+        cudaError_t e = cudaMemsetAsync(w + qd * 2 * plane, 0, plane * sizeof(fix_t), st);
+        if (e != cudaSuccess) return cuda_check(e, "memset fixed-point sums");
+    }
+    return LCB_OK;
 }
 
 static int grid_for(int64_t n, int threads)
@@ -1010,8 +1028,9 @@ static int deposit_fixed(int64_t n_per_sort, int n_sorts, int N, double h, int p
     LCB_REQUIRE(workspace && workspace_bytes >= (size_t)8 * plane * sizeof(fix_t),
                 "deposit workspace too small");
     fix_t *w = static_cast<fix_t *>(workspace);
-    cudaError_t e = cudaMemsetAsync(w, 0, 8 * plane * sizeof(fix_t), st);
-    if (e != cudaSuccess) return cuda_check(e, "memset fixed-point sums");
+    int rc = clear_fixed(w, plane, n_sorts, st);
+    if (rc) return rc;
+    cudaError_t e;
     if (n_per_sort > 0) {
         const dim3 grid((particles_side + DEP_TJ - 1) / DEP_TJ,
                         (particles_side + 1 + DEP_TI - 1) / DEP_TI, n_sorts);   // spare tile row
@@ -1028,8 +1047,8 @@ static int deposit_fixed(int64_t n_per_sort, int n_sorts, int N, double h, int p
             w, w + 2 * plane, w + 4 * plane, w + 6 * plane, err);
         LCB_LAUNCH_CHECK("k_deposit_tiled<fixed>");
     }
-    k_fix_finish<<<grid_for(2 * plane, 256), 256, 0, st>>>(plane, n_sorts, w, ro_initial, ro,
-                                                           jx, jy, jz);
+    k_fix_finish<<<grid_for(plane, 256), 256, 0, st>>>(plane, n_sorts, w, ro_initial, ro,
+                                                       jx, jy, jz);
     LCB_LAUNCH_CHECK("k_fix_finish");
     return LCB_OK;
 }
@@ -1149,15 +1168,15 @@ extern "C" int lcb_plasma_move_deposit(const lcb_move_deposit_args *a, void *str
         LCB_REQUIRE(a->workspace && a->workspace_bytes >= lcb_plasma_deposit_workspace_bytes(N, a->precision),
                     "deposit workspace too small");
         fix_t *w = static_cast<fix_t *>(a->workspace);
-        cudaError_t e = cudaMemsetAsync(w, 0, 8 * plane * sizeof(fix_t), st);
-        if (e != cudaSuccess) return cuda_check(e, "memset fixed-point sums");
+        const int rc0 = clear_fixed(w, plane, a->n_sorts, st);
+        if (rc0) return rc0;
         if (a->n_per_sort > 0) {
             fix_t *const out[4] = {w, w + 2 * plane, w + 4 * plane, w + 6 * plane};
             const int rc = dispatch_move_deposit_pair<float>(a, out, st);
             if (rc) return rc;
             LCB_LAUNCH_CHECK("k_move_deposit_pair<float>");
         }
-        k_fix_finish<<<grid_for(2 * plane, 256), 256, 0, st>>>(
+        k_fix_finish<<<grid_for(plane, 256), 256, 0, st>>>(
             plane, a->n_sorts, w, a->ro_initial, a->ro, a->jx, a->jy, a->jz);
         LCB_LAUNCH_CHECK("k_fix_finish");
         return LCB_OK;
