@@ -479,7 +479,6 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
     const int m0 = blockIdx.y * I8_BM, n0 = blockIdx.x * BN;
     if (m0 >= M || n0 >= N) return;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int ea = operand_exp(g.amax_a), eb = operand_exp(g.amax_b);
     const int KT = ntiles(K, TL_K);
     // this CTA's tile rows of A and tile column of B
     const uint8_t *At = reinterpret_cast<const uint8_t *>(g.A) + (int64_t)blockIdx.y * KT * I8_A_SLICE;
@@ -500,6 +499,10 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const unsigned tmem = *tslot;
     const unsigned idesc = i8_idesc<BN>();
+    // the prologue above overlaps the predecessor's tail (programmatic launch)
+    pdl_wait();
+    pdl_trigger();
+    const int ea = operand_exp(g.amax_a), eb = operand_exp(g.amax_b);
 
     // epilogue layout: warp w stores TMEM lanes 32 (w % 4) .. + 31 (tile rows)
     // and columns CW (w / 4) .. + CW - 1; pass `it` of a lane covers element
@@ -697,6 +700,8 @@ template <typename T>
 __global__ void __launch_bounds__(FOLD_THREADS) k_fold_slices(const __grid_constant__ FoldBatch<T> fb)
 {
     constexpr int NS = Slices<T>::n;
+    pdl_wait();
+    pdl_trigger();
     const FoldDesc<T> &f = fb.d[blockIdx.z];
     const int R = f.R, C = f.C, ldc = ld2(C);
     if (fb.clear && blockIdx.x == 0 && blockIdx.z == 0 && threadIdx.x < NPROB)
@@ -842,6 +847,8 @@ template <typename T>
 __global__ void __launch_bounds__(RHS_TX * RHS_TY)
 k_fields_rhs(RhsArgs a, T *X0, T *X1, T *X2, T *X3, T *X4, T *X5, T *X6)
 {
+    pdl_wait();
+    pdl_trigger();
     __shared__ double s_ro[RHS_TY + 2][RHS_TX + 2], s_jz[RHS_TY + 2][RHS_TX + 2];
     __shared__ double s_jx[RHS_TY + 2][RHS_TX + 2], s_jy[RHS_TY + 2][RHS_TX + 2];
     const int N = a.N;
@@ -891,6 +898,15 @@ k_fields_rhs(RhsArgs a, T *X0, T *X1, T *X2, T *X3, T *X4, T *X5, T *X6)
     }
 }
 
+// Zero the per-problem operand maxima (a kernel rather than a memset, so that
+// the chain of programmatic launches stays unbroken).
+__global__ void k_clear_maxima(unsigned *m)
+{
+    pdl_wait();
+    pdl_trigger();
+    if (threadIdx.x < NPROB) m[threadIdx.x] = 0u;
+}
+
 // Bz mean removal and half average, plus the Dirichlet edges of the other
 // planes (the reference pads its inner solutions with zeros).
 struct FinishArgs {
@@ -903,6 +919,7 @@ struct FinishArgs {
 
 __global__ void __launch_bounds__(256) k_fields_finish(FinishArgs a)
 {
+    pdl_wait();
     const int N = a.N;
     const int64_t plane = (int64_t)N * N;
     const double mean = *a.bz_sum / (double)plane;
@@ -998,7 +1015,8 @@ static int launch_i8(const GemmBatch<T> &b, int nsub, int maxM, int maxN, cudaSt
         attr = true;
     }
     dim3 grid((maxN + BN - 1) / BN, (maxM + I8_BM - 1) / I8_BM, nsub);
-    k_gemm_i8<T, BN, EPI><<<grid, 256, Cfg::smem, st>>>(b);
+    const cudaError_t e = launch_after(k_gemm_i8<T, BN, EPI>, grid, dim3(256), Cfg::smem, st, b);
+    if (e != cudaSuccess) return cuda_check(e, "i8 gemm launch");
     return LCB_OK;
 }
 
@@ -1052,7 +1070,8 @@ static int run_fold(T *const *src, T *const *dst, const int *probs, int np, cons
         ? (int64_t)ntiles(he, TL_K) * TL_K * ntiles(N, TL_N) * TL_N * 2 / 4
         : (int64_t)ntiles(N, TL_M) * TL_M * ntiles(he, TL_K) * TL_K * 2 / 4;
     dim3 grid((unsigned)((words + FOLD_THREADS - 1) / FOLD_THREADS), 1u, np);
-    k_fold_slices<T><<<grid, FOLD_THREADS, 0, st>>>(fb);
+    const cudaError_t e = launch_after(k_fold_slices<T>, grid, dim3(FOLD_THREADS), 0, st, fb);
+    if (e != cudaSuccess) return cuda_check(e, "fold launch");
     LCB_LAUNCH_CHECK("k_fold_slices");
     return LCB_OK;
 }
@@ -1091,14 +1110,16 @@ static int solve(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st
     unsigned *cur_mx = nullptr;
     r.amax_out = mx0;
     if (rec) {
-        cudaError_t e = cudaMemsetAsync(mx0, 0, NPROB * sizeof(unsigned), st);
+        cudaError_t e = launch_after(k_clear_maxima, dim3(1), dim3(32), 0, st, mx0);
         if (e != cudaSuccess) return cuda_check(e, "clear maxima");
+        count_launch();
     }
     {
         dim3 grid((N + RHS_TX - 1) / RHS_TX, (N + RHS_TY - 1) / RHS_TY);
-        k_fields_rhs<T><<<grid, dim3(RHS_TX, RHS_TY), 0, st>>>(
-            r, w.S1[0], w.S1[1], w.S1[2], w.S1[3], w.S1[4], w.S1[5], w.S1[6]);
-        LCB_LAUNCH_CHECK("k_fields_rhs");
+        cudaError_t e = launch_after(k_fields_rhs<T>, grid, dim3(RHS_TX, RHS_TY), 0, st, r,
+                                     w.S1[0], w.S1[1], w.S1[2], w.S1[3], w.S1[4], w.S1[5], w.S1[6]);
+        if (e != cudaSuccess) return cuda_check(e, "rhs launch");
+        count_launch();
     }
 
     // Per problem: rows x cols of X; the left operator (S or C) acts along
@@ -1223,7 +1244,8 @@ static int solve(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st
     {
         const int64_t tot = (int64_t)N * N;
         const int blocks = (int)((tot + 255) / 256);
-        k_fields_finish<<<blocks, 256, 0, st>>>(fa);
+        const cudaError_t e = launch_after(k_fields_finish, dim3(blocks), dim3(256), 0, st, fa);
+        if (e != cudaSuccess) return cuda_check(e, "fields finish launch");
         LCB_LAUNCH_CHECK("k_fields_finish");
     }
     return LCB_OK;

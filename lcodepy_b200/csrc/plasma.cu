@@ -588,6 +588,10 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
                   double *pz_f, typename StageAcc<FT>::type *ro, typename StageAcc<FT>::type *jx,
                   typename StageAcc<FT>::type *jy, typename StageAcc<FT>::type *jz, int *err)
 {
+    // launched after its predecessor's tail (programmatic launch): no global
+    // memory access before the wait
+    pdl_wait();
+    pdl_trigger();
     constexpr bool MIXED = sizeof(FT) == 4;
     typedef typename StageAcc<FT>::type Acc;
     static_assert(DEP_PPT == 2, "a thread owns two particles");
@@ -942,11 +946,13 @@ static int launch_move_deposit_pair(const lcb_move_deposit_args *a, dim3 grid,
         attr = true;
     }
     const lcb_plasma_particles &p = a->prev, &f = a->full;
-    k_move_deposit_pair<FT, WX, WY, FIRST><<<grid, DEP_THREADS, sm, st>>>(
+    const cudaError_t e = launch_after(
+        k_move_deposit_pair<FT, WX, WY, FIRST>, grid, dim3(DEP_THREADS), sm, st,
         a->n_per_sort, a->particles_side, a->grid_steps, a->h, a->xi_step, a->boundary,
         a->fields[0], a->fields[1], a->fields[2], a->fields[3], a->fields[4], a->fields[5],
         p.x_init, p.y_init, p.x_offt, p.y_offt, p.px, p.py, p.pz, p.q, p.m,
         f.q, f.x_offt, f.y_offt, f.px, f.py, f.pz, out[0], out[1], out[2], out[3], a->err);
+    if (e != cudaSuccess) return cuda_check(e, "move_deposit launch");
     return LCB_OK;
 }
 
@@ -973,6 +979,7 @@ __global__ void k_fix_finish(int64_t plane, int n_sorts, const fix_t *__restrict
                              const double *__restrict__ ro_initial, double *ro, double *jx,
                              double *jy, double *jz)
 {
+    pdl_wait();
     double *outs[4] = {ro, jx, jy, jz};
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < plane;
          t += (int64_t)gridDim.x * blockDim.x) {
@@ -991,19 +998,39 @@ __global__ void k_fix_finish(int64_t plane, int n_sorts, const fix_t *__restrict
     }
 }
 
-// Zero the columns of the fixed-point sums that the deposit adds to: all
-// eight planes with two sorts, else the first column of each quantity.
+// Zero four regions of n 8-byte words each (one kernel in the stream's chain
+// of programmatic launches, where a memset would break it).
+__global__ void __launch_bounds__(256) k_zero4(uint64_t *r0, uint64_t *r1, uint64_t *r2, uint64_t *r3,
+                                               int64_t n)
+{
+    pdl_wait();
+    pdl_trigger();
+    uint64_t *r[4] = {r0, r1, r2, r3};
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) r[q][t] = 0ull;
+    }
+}
+
+static int grid_for(int64_t n, int threads);
+
+static int zero4(void *r0, void *r1, void *r2, void *r3, int64_t n, cudaStream_t st)
+{
+    const cudaError_t e = launch_after(k_zero4, dim3(grid_for(n, 256)), dim3(256), 0, st,
+                                       static_cast<uint64_t *>(r0), static_cast<uint64_t *>(r1),
+                                       static_cast<uint64_t *>(r2), static_cast<uint64_t *>(r3), n);
+    if (e != cudaSuccess) return cuda_check(e, "zero launch");
+    count_launch();
+    return LCB_OK;
+}
+
+// Zero the columns of the fixed-point sums that the deposit adds to (the
+// first column of each quantity, both with two sorts).
 static int clear_fixed(fix_t *w, size_t plane, int n_sorts, cudaStream_t st)
 {
-    if (n_sorts > 1) {
-        cudaError_t e = cudaMemsetAsync(w, 0, 8 * plane * sizeof(fix_t), st);
-        return e != cudaSuccess ? cuda_check(e, "memset fixed-point sums") : LCB_OK;
-    }
-    for (int qd = 0; qd < 4; qd++) {
-        cudaError_t e = cudaMemsetAsync(w + qd * 2 * plane, 0, plane * sizeof(fix_t), st);
-        if (e != cudaSuccess) return cuda_check(e, "memset fixed-point sums");
-    }
-    return LCB_OK;
+    const int64_t n = (int64_t)(n_sorts > 1 ? 2 : 1) * plane;
+    return zero4(w, w + 2 * plane, w + 4 * plane, w + 6 * plane, n, st);
 }
 
 static int grid_for(int64_t n, int threads)
@@ -1047,9 +1074,10 @@ static int deposit_fixed(int64_t n_per_sort, int n_sorts, int N, double h, int p
             w, w + 2 * plane, w + 4 * plane, w + 6 * plane, err);
         LCB_LAUNCH_CHECK("k_deposit_tiled<fixed>");
     }
-    k_fix_finish<<<grid_for(plane, 256), 256, 0, st>>>(plane, n_sorts, w, ro_initial, ro,
-                                                       jx, jy, jz);
-    LCB_LAUNCH_CHECK("k_fix_finish");
+    e = launch_after(k_fix_finish, dim3(grid_for(plane, 256)), dim3(256), 0, st, (int64_t)plane,
+                     n_sorts, (const fix_t *)w, ro_initial, ro, jx, jy, jz);
+    if (e != cudaSuccess) return cuda_check(e, "fix finish launch");
+    count_launch();
     return LCB_OK;
 }
 
@@ -1176,14 +1204,16 @@ extern "C" int lcb_plasma_move_deposit(const lcb_move_deposit_args *a, void *str
             if (rc) return rc;
             LCB_LAUNCH_CHECK("k_move_deposit_pair<float>");
         }
-        k_fix_finish<<<grid_for(plane, 256), 256, 0, st>>>(
-            plane, a->n_sorts, w, a->ro_initial, a->ro, a->jx, a->jy, a->jz);
-        LCB_LAUNCH_CHECK("k_fix_finish");
+        const cudaError_t e = launch_after(k_fix_finish, dim3(grid_for(plane, 256)), dim3(256), 0, st,
+                                           (int64_t)plane, a->n_sorts, (const fix_t *)w,
+                                           a->ro_initial, a->ro, a->jx, a->jy, a->jz);
+        if (e != cudaSuccess) return cuda_check(e, "fix finish launch");
+        count_launch();
         return LCB_OK;
     }
-    for (double *p : {a->ro, a->jx, a->jy, a->jz}) {
-        cudaError_t e = cudaMemsetAsync(p, 0, 2 * plane * sizeof(double), st);
-        if (e != cudaSuccess) return cuda_check(e, "memset currents");
+    {
+        const int rc0 = zero4(a->ro, a->jx, a->jy, a->jz, 2 * (int64_t)plane, st);
+        if (rc0) return rc0;
     }
     if (a->n_per_sort > 0) {
         double *const out[4] = {a->ro, a->jx, a->jy, a->jz};
