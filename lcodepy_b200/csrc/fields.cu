@@ -281,6 +281,9 @@ struct GemmDesc {
     // mixed precision: A and B are four tiled int8 slice planes (A role and
     // B role); a_plane / b_plane are the plane strides in bytes
     int a_plane, b_plane;
+    // which operand is a transform block (1: A, 2: B), whose copies may be
+    // issued before the predecessor kernel has finished
+    int const_op;
 };
 
 enum Epi { EPI_STORE = 0, EPI_SCALE = 1, EPI_FIELD = 2 };
@@ -443,13 +446,17 @@ __device__ __forceinline__ double epi_apply(const GemmBatch<T> &b, const GemmDes
 
 template <int NS, int BN>
 struct I8Cfg {
-    // a CTA covers BN columns: a whole 64-wide B tile or, for BN = 32, the
-    // contiguous half of one (its N core-matrix groups 0-1 or 2-3)
-    static_assert(TL_N % BN == 0 && BN % 16 == 0, "tile width");
+    // a CTA covers BN columns: two consecutive 64-wide B tiles (BN = 128,
+    // one CTA per SM, all of tensor memory), a whole one (BN = 64, two CTAs
+    // per SM) or, for BN = 32, the contiguous half of one (its N core-matrix
+    // groups 0-1 or 2-3)
+    static_assert((TL_N % BN == 0 || BN == 2 * TL_N) && BN % 16 == 0, "tile width");
     static constexpr int B_SLICE = I8_BK * BN;                         // bytes
     static constexpr int STAGE = NS * (I8_A_SLICE + B_SLICE);          // bytes
-    static constexpr int ST = 4 * STAGE <= 100 * 1024 ? 4 : 2;         // pipeline stages
+    static constexpr int ST = BN > TL_N ? 6 : (4 * STAGE <= 100 * 1024 ? 4 : 2);  // pipeline stages
     static constexpr int TMEM_COLS = NS * BN;                          // power of two
+    static constexpr int THREADS = BN > TL_N ? 512 : 256;              // 16 or 8 warps
+    static constexpr int CW = BN / (THREADS / 128);                    // epilogue columns per warp
     static constexpr size_t smem = (size_t)ST * STAGE + 128;   // + 2 ST + 1 barriers, TMEM slot
 };
 
@@ -460,14 +467,16 @@ __device__ __forceinline__ void bulk_g2s(unsigned dst, const void *src, unsigned
 }
 
 template <typename T, int BN, int EPI>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(I8Cfg<Slices<T>::n, BN>::THREADS, 512 / I8Cfg<Slices<T>::n, BN>::TMEM_COLS)
 k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
 {
     constexpr int NS = Slices<T>::n;
     using Cfg = I8Cfg<NS, BN>;
     constexpr int ST = Cfg::ST;
+    constexpr int CW = Cfg::CW;           // epilogue columns per warp
     static_assert(Cfg::TMEM_COLS == 256 || Cfg::TMEM_COLS == 512, "tensor memory columns");
-    static_assert(8 * 32 * (BN / 2 + 1) * sizeof(T) <= (size_t)ST * Cfg::STAGE, "epilogue staging");
+    static_assert(Cfg::THREADS / 32 * 32 * (CW + 1) * sizeof(T) <= (size_t)ST * Cfg::STAGE,
+                  "epilogue staging");
     extern __shared__ __align__(1024) uint8_t i8sm[];
     uint64_t *full = reinterpret_cast<uint64_t *>(i8sm + ST * Cfg::STAGE);   // [ST] copies landed
     uint64_t *done = full + ST;                                             // [ST] MMAs finished
@@ -484,6 +493,9 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
     const uint8_t *At = reinterpret_cast<const uint8_t *>(g.A) + (int64_t)blockIdx.y * KT * I8_A_SLICE;
     const uint8_t *Bt = reinterpret_cast<const uint8_t *>(g.B) + (int64_t)(n0 / TL_N) * KT * (TL_K * TL_N) +
                         ((n0 % TL_N) >> 4) * 512;
+    // BN = 128: the second B tile column (or the first again past the last
+    // one; its products land in columns that are never stored)
+    const uint8_t *Bt2 = (n0 / TL_N + 1) < ntiles(N, TL_N) ? Bt + (int64_t)KT * (TL_K * TL_N) : Bt;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -499,9 +511,46 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const unsigned tmem = *tslot;
     const unsigned idesc = i8_idesc<BN>();
+
+    // Stage copies (lane 0 of warp 0): part 1 = A slices, part 2 = B slices,
+    // part 3 = both; the stage's barrier expects all of its bytes once.
+    auto load = [&](int kt, int part, bool expect) {
+        if (warp != 0 || lane != 0) return;
+        const int buf = kt % ST;
+        const unsigned sA = smem_u32(i8sm + buf * Cfg::STAGE);
+        const unsigned sB = sA + NS * I8_A_SLICE;
+        const unsigned mb = smem_u32(full + buf);
+        if (expect)
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;"
+                         :: "r"((unsigned)Cfg::STAGE), "r"(mb) : "memory");
+#pragma unroll
+        for (int i = 0; i < NS; i++) {
+            if (part & 1)
+                bulk_g2s(sA + i * I8_A_SLICE, At + (int64_t)i * g.a_plane + (int64_t)kt * I8_A_SLICE,
+                         I8_A_SLICE, mb);
+            if (part & 2) {
+                if constexpr (BN > TL_N) {
+                    constexpr int HB = TL_K * TL_N;   // one 64-wide tile slice
+                    bulk_g2s(sB + i * Cfg::B_SLICE, Bt + (int64_t)i * g.b_plane + (int64_t)kt * HB, HB, mb);
+                    bulk_g2s(sB + i * Cfg::B_SLICE + HB, Bt2 + (int64_t)i * g.b_plane + (int64_t)kt * HB, HB,
+                             mb);
+                } else {
+                    bulk_g2s(sB + i * Cfg::B_SLICE, Bt + (int64_t)i * g.b_plane + (int64_t)kt * (TL_K * TL_N),
+                             Cfg::B_SLICE, mb);
+                }
+            }
+        }
+    };
+    // the first stages' transform-block copies go out before the wait: the
+    // blocks are written once, when the operators are built
+    const int npre = ST < KT ? ST : KT;
+    const int cpart = g.const_op, dpart = 3 - cpart;
+    if (cpart)
+        for (int kt = 0; kt < npre; kt++) load(kt, cpart, true);
     // the prologue above overlaps the predecessor's tail (programmatic launch)
     pdl_wait();
     pdl_trigger();
+    for (int kt = 0; kt < npre; kt++) load(kt, cpart ? dpart : 3, !cpart);
     const int ea = operand_exp(g.amax_a), eb = operand_exp(g.amax_b);
 
     // epilogue layout: warp w stores TMEM lanes 32 (w % 4) .. + 31 (tile rows)
@@ -509,7 +558,6 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
     // it * 32 + lane of the warp's 32 x CW block (lanes along a row).  The
     // values the epilogue reads (spectral factors, previous fields) are
     // loaded here, so that their latency hides behind the main loop.
-    constexpr int CW = BN / 2;            // columns per warp
     const int rq = warp & 3, ch = warp >> 2;
     double pre[CW];
 #pragma unroll
@@ -524,23 +572,6 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
         // warp 0 streams the stages (eight bulk copies each: four A and four
         // B slice tiles) and issues the MMAs from lane 0; the whole warp
         // follows the loop so that lane 0 never diverges from idle lanes
-        auto load = [&](int kt) {
-            if (lane != 0) return;
-            const int buf = kt % ST;
-            const unsigned sA = smem_u32(i8sm + buf * Cfg::STAGE);
-            const unsigned sB = sA + NS * I8_A_SLICE;
-            const unsigned mb = smem_u32(full + buf);
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;"
-                         :: "r"((unsigned)Cfg::STAGE), "r"(mb) : "memory");
-#pragma unroll
-            for (int i = 0; i < NS; i++) {
-                bulk_g2s(sA + i * I8_A_SLICE, At + (int64_t)i * g.a_plane + (int64_t)kt * I8_A_SLICE,
-                         I8_A_SLICE, mb);
-                bulk_g2s(sB + i * Cfg::B_SLICE, Bt + (int64_t)i * g.b_plane + (int64_t)kt * (TL_K * TL_N),
-                         Cfg::B_SLICE, mb);
-            }
-        };
-        for (int kt = 0; kt < ST && kt < KT; kt++) load(kt);
         for (int kt = 0; kt < KT; kt++) {
             const int buf = kt % ST;
             ok &= mbar_wait(smem_u32(full + buf), (kt / ST) & 1);
@@ -574,7 +605,7 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
             const int nxt = kt - 1 + ST;
             if (kt >= 1 && nxt < KT) {
                 ok &= mbar_wait(smem_u32(done + (kt - 1) % ST), ((kt - 1) / ST) & 1);
-                load(nxt);
+                load(nxt, 3, true);
             }
         }
     }
@@ -637,7 +668,7 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
                      :: "r"(tmem), "r"(Cfg::TMEM_COLS) : "memory");
-    if (EPI == EPI_FIELD && batch.out[g.prob].kind == 3) bz_reduce<256>(part, batch.out[g.prob].bz_sum);
+    if (EPI == EPI_FIELD && batch.out[g.prob].kind == 3) bz_reduce<Cfg::THREADS>(part, batch.out[g.prob].bz_sum);
 }
 
 // ---------------------------------------------------------------------------
@@ -1002,8 +1033,9 @@ static Work<T> carve(void *ws, int N)
 template <typename T, int EPI>
 static int launch_i8(const GemmBatch<T> &b, int nsub, int maxM, int maxN, cudaStream_t st)
 {
-    // 256 tensor-memory columns per CTA (NS accumulators x BN) so that two
-    // CTAs share an SM: 64-wide tiles for four slices, 32-wide for eight
+    // 256 tensor-memory columns per CTA (NS accumulators x BN), two CTAs per
+    // SM: 64-wide tiles for four slices, 32-wide for eight (128-wide tiles,
+    // one CTA per SM, read less operand data but ran no faster)
     constexpr int BN = Slices<T>::n == 8 ? 32 : 64;
     using Cfg = I8Cfg<Slices<T>::n, BN>;
     static bool attr = false;
@@ -1015,7 +1047,7 @@ static int launch_i8(const GemmBatch<T> &b, int nsub, int maxM, int maxN, cudaSt
         attr = true;
     }
     dim3 grid((maxN + BN - 1) / BN, (maxM + I8_BM - 1) / I8_BM, nsub);
-    const cudaError_t e = launch_after(k_gemm_i8<T, BN, EPI>, grid, dim3(256), Cfg::smem, st, b);
+    const cudaError_t e = launch_after(k_gemm_i8<T, BN, EPI>, grid, dim3(Cfg::THREADS), Cfg::smem, st, b);
     if (e != cudaSuccess) return cuda_check(e, "i8 gemm launch");
     return LCB_OK;
 }
@@ -1151,6 +1183,7 @@ static int solve(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st
                 d.lda = par ? ld2(ho) : ld2(he);
                 const int id = rightS[p] ? (par ? OP_SOT : OP_SET) : (par ? OP_COT : OP_CET);
                 d.B = op(id); d.ldb = (int)L.ld[id];
+                d.const_op = 2;
                 d.M = rows[p]; d.K = par ? ho : he; d.N = par ? ho : he;
                 d.rmul = 1; d.radd = 0; d.cmul = 2; d.cadd = par;
                 d.C = w.S1[p]; d.ldc = ld2(C); d.prob = p;
@@ -1177,6 +1210,7 @@ static int solve(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st
                 memset(&d, 0, sizeof(d));
                 const int id = leftS[p] ? (par ? OP_SO : OP_SE) : (par ? OP_CO : OP_CE);
                 d.A = op(id); d.lda = (int)L.ld[id];
+                d.const_op = 1;
                 d.B = w.S2[p] + (par ? (int64_t)he * ld2(cols[p]) : 0); d.ldb = ld2(cols[p]);
                 d.M = par ? ho : he; d.K = par ? ho : he; d.N = cols[p];
                 d.rmul = 2; d.radd = par; d.cmul = 1; d.cadd = 0;
