@@ -365,7 +365,8 @@ def plain_ms_per_step(N, precision="fp64", n_steps=120, skip=20, beam=None):
     else:
         import dataclasses
         beam = dataclasses.replace(beam, r_max=min(beam.r_max, 0.4 * cfg['window-width']))
-        src, drain = BeamSource(conf, beam.particles(cfg['xi-step']), dev), BeamDrain(conf, dev)
+        src = BeamSource(conf, beam.device_beam(cfg['xi-step'], dev), dev)
+        drain = BeamDrain(conf, dev)
     ps.step_dt(cfg['xi-step'], src, drain, 1.0, [], step_hook=hook)
     torch.cuda.synchronize()
     return ev[skip].elapsed_time(ev[n_steps]) / (n_steps - skip)

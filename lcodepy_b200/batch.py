@@ -54,8 +54,9 @@ class GaussianDriver:
 @dataclasses.dataclass
 class BeamDriver:
     """A non-rigid electron driver: n macroparticles, bi-Gaussian (sigma_r,
-    sigma_z) around xi0, peak density `amplitude` (in n0; the beam charge is
-    negative), gamma with a relative spread, normalised emittance; seeded."""
+    sigma_z) around xi0 (cut to 2 xi0 < xi < 0 and r < r_max), peak density
+    `amplitude` (in n0; the beam charge is negative), gamma with a relative
+    spread, normalised emittance; generated on the device from `seed`."""
     n: int = 100_000
     amplitude: float = 0.1
     sigma_r: float = 1.0
@@ -67,10 +68,48 @@ class BeamDriver:
     seed: int = 0
     r_max: float = 4.0        # radial cut (keep it inside the window)
 
+    def device_beam(self, dxi: float, device=None):
+        """The beam generated on the device (seeded Philox stream of
+        torch.Generator), sorted by xi descending, as BeamParticles: the
+        distribution of bigaussian_beam in milliseconds instead of the host's
+        tenths of a second, so that admitting a request does not stall the
+        server loop."""
+        from .beam3d import BeamParticles
+        dev = device or torch.device("cuda", torch.cuda.current_device())
+        g = torch.Generator(device=dev)
+        g.manual_seed(int(self.seed))
+        f64 = dict(dtype=torch.float64, device=dev, generator=g)
+        xi = torch.randn(2 * self.n, **f64) * self.sigma_z + self.xi0
+        xi = xi[(xi < 0) & (xi > 2 * self.xi0)][:self.n]
+        m = xi.numel()
+        cut = 1 - math.exp(-self.r_max ** 2 / (2 * self.sigma_r ** 2))
+        r = self.sigma_r * torch.sqrt(-2 * torch.log1p(-torch.rand(m, **f64) * cut))
+        phi = torch.rand(m, **f64) * (2 * math.pi)
+        sp = self.emittance / self.sigma_r
+        b = BeamParticles(dev)
+        b.xi = xi
+        b.x, b.y = r * torch.cos(phi), r * torch.sin(phi)
+        b.px = torch.randn(m, **f64) * sp
+        b.py = torch.randn(m, **f64) * sp
+        b.pz = torch.randn(m, **f64) * (self.gamma * self.espread) + self.gamma
+        b.q_m = torch.full((m,), -1.0, dtype=torch.float64, device=dev)
+        q_total = (-self.amplitude * (math.sqrt(2 * math.pi) * self.sigma_z)
+                   * (2 * math.pi * self.sigma_r ** 2) / dxi)
+        b.q_norm = torch.full((m,), q_total / max(m, 1), dtype=torch.float64, device=dev)
+        b.id = torch.arange(1, m + 1, dtype=torch.int64, device=dev)
+        b.dt = torch.zeros_like(b.q_norm)
+        b.remaining_steps = torch.zeros_like(b.id)
+        b.xi_sorted()
+        return b
+
     def particles(self, dxi: float) -> np.ndarray:
-        return bigaussian_beam(self.n, self.seed, self.sigma_r, self.sigma_z, self.xi0,
-                               self.gamma, self.espread, self.emittance, -self.amplitude, dxi,
-                               self.r_max)
+        """The same beam as a host particle_dtype3d array (for beam files)."""
+        from .beam_generator import particle_dtype3d
+        b = self.device_beam(dxi)
+        out = np.zeros(b.xi.numel(), dtype=particle_dtype3d)
+        for k in ('xi', 'x', 'y', 'px', 'py', 'pz', 'q_m', 'q_norm', 'id'):
+            out[k] = getattr(b, k).cpu().numpy()
+        return out
 
 
 def bigaussian_beam(n=1_000_000, seed=2024, sigma_r=0.5, sigma_z=1.0, xi0=-3.0,
@@ -254,7 +293,7 @@ class BeamMember(Member):
             self.solver.init_state(cfg.getfloat('time-step'))
             self.solver.capture_on_stream = True
             self.bc = BeamCalculator(cfg, self.device)
-            self.source = BeamSource(cfg, driver.particles(self.dxi), self.device)
+            self.source = BeamSource(cfg, driver.device_beam(self.dxi, self.device), self.device)
             self.bc.start_time_step(self.source)
             self.bc.layout_first(0)
             self.counter = torch.zeros(1, dtype=torch.int64, device=self.device)

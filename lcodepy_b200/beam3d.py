@@ -240,6 +240,8 @@ class BeamCalculator:
         # device counters: fell A, fell B, drain, lost
         self.counts = torch.zeros(4, dtype=torch.int64, device=self.device)
         self.cap = 0
+        self._plane_ptrs = [self.planes[k].data_ptr() for k in range(3)]
+        self._step_args_cache = {}   # per fell buffer parity; reset with the buffers
 
     def _ensure(self, n_total, max_layer):
         cap = max(n_total, 1)
@@ -247,6 +249,7 @@ class BeamCalculator:
         if cap <= self.cap and stage <= self.stage_cap:
             return
         self.cap, self.stage_cap = cap, stage
+        self._step_args_cache = {}
         self.drain = BeamParticles(self.device, cap)
         self.lost = BeamParticles(self.device, cap)
         self.fell = [BeamParticles(self.device, cap), BeamParticles(self.device, cap)]
@@ -256,6 +259,7 @@ class BeamCalculator:
     def start_time_step(self, source: "BeamSource"):
         """Zero the planes and counters and lay out the first layer."""
         self.source = source
+        self._step_args_cache = {}
         self.bounds = source.all_layer_bounds()
         n = source.beam.size
         max_layer = max((b - a for a, b in self.bounds.values()), default=0)
@@ -316,13 +320,21 @@ class BeamCalculator:
 
     def after_plasma_step(self, i, fields_prev, fields_new):
         """Push layer i-1 (and the particles that fell from the last push)
-        between fields_prev and fields_new, then lay out layer i+1."""
+        between fields_prev and fields_new, then lay out layer i+1.  The
+        argument struct is built once per fell-buffer parity; a step only
+        sets its layer indices, ranges, planes and fields."""
         self.planes[(i + 2) % 3].zero_()
-        a = self._args(i, self.layer_bounds(i + 1), self.layer_bounds(i - 1),
-                       fields_prev, fields_new)
+        a = self._step_args_cache.get(self.fell_cur)
+        if a is None:
+            a = self._step_args_cache[self.fell_cur] = self._args(i, (0, 0), (0, 0), None, None)
+        a.layer_idx = i
         a.layout_idx = i + 1
-        a.ro0 = self.planes[(i + 1) % 3].data_ptr()
-        a.ro1 = self.planes[(i + 2) % 3].data_ptr()
+        a.layout_begin, a.layout_end = self.layer_bounds(i + 1)
+        a.move_begin, a.move_end = self.layer_bounds(i - 1)
+        a.ro0 = self._plane_ptrs[(i + 1) % 3]
+        a.ro1 = self._plane_ptrs[(i + 2) % 3]
+        a.fields_k = C.addressof(fields_prev.struct) if fields_prev is not None else None
+        a.fields_k1 = C.addressof(fields_new.struct) if fields_new is not None else None
         _lib.check(_lib.load().lcb_beam_step(C.byref(a), _lib.stream_handle()),
                    "lcb_beam_step")
         self.fell_cur = 1 - self.fell_cur
