@@ -87,4 +87,6 @@ class Arrays:
                              for k, v in self.__dict__.items() if k != "xp"})
 
     def save(self, *args, **kwargs):
-        np.savez_compressed(*args, **kwargs, **self.to_numpy().__dict__)
+        """np.savez_compressed of every array (lcode/plasma3d/data.py:31-34)."""
+        data = {k: v for k, v in self.to_numpy().__dict__.items() if k != "xp"}
+        np.savez_compressed(*args, **kwargs, **data)

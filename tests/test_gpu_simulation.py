@@ -175,3 +175,40 @@ def test_fused_stage_matches_separate_kernels(extra):
     for s in p0:
         for k in ("x_offt", "px", "q"):
             assert rel_err(getattr(p1[s], k).cpu().numpy(), getattr(p0[s], k).cpu().numpy()) < tol
+
+
+def test_device_diagnostics_record_the_run(tmp_path, monkeypatch):
+    """FXiDiag / SliceDiag / ParticlesDiag attached to the drop-in Simulation:
+    the on-axis Ez they write equals the solver's own record, the slices are
+    the final fields, and the snapshots hold the final particles."""
+    from lcodepy_b200.diagnostics import (FXiDiag, FXiType, ParticlesDiag, SliceDiag,
+                                          SliceType, SliceValue)
+    monkeypatch.chdir(tmp_path)
+    fxi = FXiDiag(output_period=1, f_xi=FXiType.Ez | FXiType.ne | FXiType.Sf)
+    sl = SliceDiag(SliceType.XI_X, slice_value=SliceValue.Ez, output_period=1)
+    pd = ParticlesDiag(save_plasma=True, output_period=1, saving_xi_period=1.0)
+    sim = Simulation(config=cfg(**{'rigid-beam': True}), beam_parameters=rigid_driver,
+                     diagnostics=[fxi, sl, pd], runas_filename='')
+    sim.step(1)
+    ps = sim.push_solver
+    ez = ps.ez_axis.cpu().numpy()
+    diag = tmp_path / 'diagnostics'
+
+    def one(pattern):
+        files = sorted(diag.glob(pattern))
+        assert len(files) == 1, files
+        return files[0]
+
+    with np.load(one('f_xi_*.npz')) as z:
+        assert np.array_equal(z['Ez'], ez)
+        assert z['xi'].shape == ez.shape and z['ne'].shape == ez.shape and z['Sf'].shape == ez.shape
+    _, fields, _ = ps._plasmastate
+    N = fields.Ez.shape[0]
+    with np.load(one('slice_*.npz')) as z:
+        n = z['x'].size   # the reference's default x range: the first N - 1 rows
+        assert z['Ez'].shape == (ez.size, n) and n == N - 1
+        assert np.array_equal(z['Ez'][-1], fields.Ez[:n, N // 2].cpu().numpy())
+    particles, _, _ = ps._plasmastate
+    with np.load(one('plasma_electrons_*.npz')) as z:
+        assert np.array_equal(z['px'], particles['electrons'].px.cpu().numpy())
+    assert len(list((diag / 'snapshots').glob('plasma_electrons_*.npz'))) >= 1
