@@ -663,8 +663,8 @@ def main():
 # capture of the small case of the same workload (N=513, 11 xi steps):
 # compute_fields counts its four tensor-core waves, move_deposit the fused
 # kernel of a non-first stage.
-NCU_TRAFFIC = {("compute_fields", "fp64"): 85.5e6, ("compute_fields", "mixed"): 43.6e6,
-               ("move_deposit", "fp64"): 119.5e6, ("move_deposit", "mixed"): 116.7e6}
+NCU_TRAFFIC = {("compute_fields", "fp64"): 85.1e6, ("compute_fields", "mixed"): 43.8e6,
+               ("move_deposit", "fp64"): 118.2e6, ("move_deposit", "mixed"): 115.5e6}
 
 
 def transform_flops(N):
