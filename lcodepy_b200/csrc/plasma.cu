@@ -424,6 +424,26 @@ __device__ __forceinline__ void weights4f(float x, float w[5])
 __device__ __forceinline__ void weights_of(float x, float w[5]) { weights4f(x, w); }
 __device__ __forceinline__ void weights_of(double x, double w[5]) { weights4(x, w); }
 
+// Packed FP32 pairs (sm_100 f32x2 arithmetic): two floats in one 64-bit
+// register pair, and an FMA on both lanes.
+__device__ __forceinline__ unsigned long long f32x2(float lo, float hi)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void unpack_f32x2(unsigned long long v, float &lo, float &hi)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long fma_f32x2(unsigned long long a, unsigned long long b,
+                                                        unsigned long long c)
+{
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
 // Field window in shared memory: the six field values of a cell are stored
 // together, so that one stencil point of the gather takes vector loads
 // (FP32: a float4 of Ex, Ey, Ez, Bx and a float2 of By, Bz; FP64: three
@@ -737,7 +757,38 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
         const int lx = ix[0] - 2 - wx0, ly = iy[0] - 2 - wy0;
         const bool joint = ix[0] >= 0 && ix[0] == ix[1] && iy[0] == iy[1] &&
                            lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY;
-        if (joint) {
+        if (joint && MIXED) {
+            // FP32: the window's float4 / float2 of a cell are register pairs
+            // (Ex Ey)(Ez Bx)(By Bz), accumulated with packed f32x2 FMAs
+            // (per lane the same rounding as the scalar FMAs)
+            float ax[5], ay[5], bx[5], by[5];
+            weights4f((float)xlf[0], ax); weights4f((float)ylf[0], ay);
+            weights4f((float)xlf[1], bx); weights4f((float)ylf[1], by);
+            unsigned long long A[3] = {0ull, 0ull, 0ull}, B[3] = {0ull, 0ull, 0ull};
+#pragma unroll
+            for (int a = 0; a < 5; a++) {
+#pragma unroll
+                for (int b = 0; b < 5; b++) {
+                    const float wa = ax[a] * ay[b], wb = bx[a] * by[b];
+                    const unsigned long long wa2 = f32x2(wa, wa), wb2 = f32x2(wb, wb);
+                    const int c = (lx + a) * WY + ly + b;
+                    const float4 p = reinterpret_cast<const float4 *>(sf)[c];
+                    const float2 q = reinterpret_cast<const float2 *>(sf + 16 * WSZ)[c];
+                    const unsigned long long v3[3] = {f32x2(p.x, p.y), f32x2(p.z, p.w), f32x2(q.x, q.y)};
+#pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        A[k] = fma_f32x2(v3[k], wa2, A[k]);
+                        B[k] = fma_f32x2(v3[k], wb2, B[k]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                float lo, hi;
+                unpack_f32x2(A[k], lo, hi); F0[2 * k] = (FT)lo; F0[2 * k + 1] = (FT)hi;
+                unpack_f32x2(B[k], lo, hi); F1[2 * k] = (FT)lo; F1[2 * k + 1] = (FT)hi;
+            }
+        } else if (joint) {
             FT ax[5], ay[5], bx[5], by[5];
             weights_of(xlf[0], ax); weights_of(ylf[0], ay);
             weights_of(xlf[1], bx); weights_of(ylf[1], by);
