@@ -79,8 +79,6 @@ class Simulation:
         self.__pull_config()
         if self.runas_filename:
             self.__config.dump(self.runas_filename)
-        if self.external_plasmastate:
-            raise NotImplementedError("external plasma states are not supported yet")
         if self.__rigid_beam:
             N_steps = 1
             print("Since the beam is rigid, the code will simulate only one time step.")
@@ -107,10 +105,21 @@ class Simulation:
             self.beam_drain = BeamDrain(self.__config, self.device)
 
         ps = self.__push_solver
+        # an external plasma state replaces the initial plasma of every time
+        # step, and the xi loop continues after its layer (simulation.py:154-165)
+        state = None
+        if self.external_plasmastate:
+            from .plasma_state import load_plasmastate
+            state = load_plasmastate(self.path_to_plasmastate, ps.plasma_solver.sort_names)
         self.current_time = self.__time_step_size
         for t_i in range(N_steps):
             ps.plasma_solver.init_state(self.current_time)
-            ps.step_dt(self.__config.getfloat('xi-step'), self.beam_source, self.beam_drain,
+            xi_start = self.__config.getfloat('xi-step')
+            if state is not None:
+                xs = ps.plasma_solver.load_state(state)
+                if xs is not None:
+                    xi_start = xs
+            ps.step_dt(xi_start, self.beam_source, self.beam_drain,
                        self.current_time, self.diagnostics_list)
             if t_i != N_steps - 1 and not self.__rigid_beam:
                 self.beam_source = BeamSource(self.__config, self.beam_drain.beam_slice(),

@@ -163,6 +163,37 @@ class Plane2d3vPlasmaSolver:
         self.cur = 0
         self.last_fields = self.fields[1]
 
+    def load_state(self, state: dict):
+        """Start from a stored plasma state (``plasma_state.load_plasmastate``)
+        instead of the initial one: particles of every sort, the previous
+        fields and currents, and the background charge if the state has it
+        (initialization.py:417-460).  Call after ``init_state``; returns the
+        state's xi_plasma_layer (None if it has none)."""
+        st0 = self.states[0]
+        n, Ns, N = st0.n_per_sort, st0.Ns, self.N
+        for si, sort in enumerate(self.sort_names):
+            rec = state["particles"][sort]
+            if rec["x_init"].shape != (Ns, Ns):
+                raise ValueError(f"plasma state '{sort}' has a {rec['x_init'].shape} lattice, "
+                                 f"this configuration {Ns} x {Ns}")
+            for k in PARTICLE_NAMES:
+                t = torch.from_numpy(np.ascontiguousarray(rec[k]).ravel()).to(self.device)
+                for s in self.states:
+                    s.t[k][si * n:(si + 1) * n] = t
+        for key, shape in (("fields", (N, N)), ("currents", (2, N, N))):
+            for k, a in state[key].items():
+                if a.shape != shape:
+                    raise ValueError(f"plasma state {key} '{k}' has shape {a.shape}, expected {shape}")
+        F = self.fields[self.cur]
+        for i, k in enumerate(FIELD_NAMES):
+            F.buf[i].copy_(torch.from_numpy(state["fields"][k]))
+        Cs = self.currents[self.cur]
+        for i, k in enumerate(CURRENT_NAMES):
+            Cs.buf[i].copy_(torch.from_numpy(state["currents"][k]))
+        if state.get("rho_initial") is not None:
+            self.ro_initial.copy_(torch.from_numpy(state["rho_initial"]))
+        return state.get("xi_plasma_layer")
+
     # -- kernels --
     def _deposit(self, st: PlasmaState, out: CurrentSet, with_background=True, n_sorts=None):
         L = _lib.load()

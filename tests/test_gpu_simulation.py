@@ -212,3 +212,37 @@ def test_device_diagnostics_record_the_run(tmp_path, monkeypatch):
     with np.load(one('plasma_electrons_*.npz')) as z:
         assert np.array_equal(z['px'], particles['electrons'].px.cpu().numpy())
     assert len(list((diag / 'snapshots').glob('plasma_electrons_*.npz'))) >= 1
+
+
+def test_resume_from_a_stored_plasma_state(tmp_path):
+    """A state stored by a diagnostic at layer k and loaded through
+    external_plasmastate continues the xi loop as the uninterrupted run.  As
+    in the reference, a resumed time step starts with a zero beam density for
+    the stored layer, so the layer is taken behind the driver (xi < -2.51)."""
+    from lcodepy_b200.plasma_state import save_plasmastate
+    path = tmp_path / "plasmastate.npz"
+    k_store = 56
+
+    class Store:
+        def pull_config(self, config):
+            self.k = 0
+
+        def after_step_dxi(self, t, xi, particles, fields, currents, rho_beam):
+            if self.k == k_store:
+                save_plasmastate(path, particles, fields, currents, xi_plasma_layer=xi)
+            self.k += 1
+
+        def dump(self, *a, **k):
+            pass
+
+    c = cfg(**{'rigid-beam': True, 'window-length': 4.0})
+    sim = Simulation(config=c, beam_parameters=rigid_driver, diagnostics=[Store()], runas_filename='')
+    sim.step(1)
+    ez_all = sim.push_solver.ez_axis.cpu().numpy()
+    sim2 = Simulation(config=c, beam_parameters=rigid_driver, runas_filename='')
+    sim2.external_plasmastate = True
+    sim2.path_to_plasmastate = str(path)
+    sim2.step(1)
+    ez_resumed = sim2.push_solver.ez_axis.cpu().numpy()
+    assert ez_resumed.shape == ez_all[k_store + 1:].shape
+    assert rel_err(ez_resumed, ez_all[k_store + 1:]) < 1e-10
