@@ -15,6 +15,9 @@ Fixtures:
   run_rigid_bg.npz     -- full xi loop, rigid driver, background ions
   run_rigid_mobile.npz -- full xi loop, rigid driver, mobile ions
   run_beam.npz         -- full xi loop, generated (non-rigid) beam, 1 time step
+  run_profile_*.npz    -- rigid driver with a channel (9 per cell) and a
+                          gaussian (1 per cell, mobile ions) transverse
+                          plasma profile (with --profiles)
   run_test1.npz        -- the reference's own 3D golden configuration
                           (tests/integration/test_3D_part.py:9-56): strided
                           final state and on-axis Ez per xi step
@@ -233,6 +236,23 @@ def main(ref_root):
     print('whole runs', time.time() - t, 's')
     if '--test1' in sys.argv:
         make_test1(lcode)
+    if '--profiles' in sys.argv:
+        make_profiles(lcode)
+
+
+def make_profiles(lcode):
+    """Transverse plasma profiles and other lattice finenesses (rigid driver)."""
+    out = run_sim(lcode, base_config(**{'rigid-beam': True, 'window-length': 1.0,
+                                        'plasma-particles-per-cell': 9,
+                                        'plasma-rshape': 'channel', 'plasma-width': 0.6,
+                                        'plasma-width-2': 0.9, 'plasma-density-2': 0.5}),
+                  rigid_driver)
+    np.savez_compressed(os.path.join(HERE, 'run_profile_channel.npz'), **out)
+    out = run_sim(lcode, base_config(**{'rigid-beam': True, 'window-length': 1.0,
+                                        'plasma-particles-per-cell': 1, 'ion-model': 'mobile',
+                                        'plasma-rshape': 'gaussian', 'plasma-width': 0.5}),
+                  rigid_driver)
+    np.savez_compressed(os.path.join(HERE, 'run_profile_gauss.npz'), **out)
 
 
 def make_test1(lcode):

@@ -60,6 +60,12 @@ def check(ref, particles, fields, currents, sorts, rel):
     ("run_rigid_bg.npz", {}, ["electrons"]),
     ("run_rigid_mobile.npz", {'ion-model': 'mobile', 'window-length': 1.0, 'xi-step': 0.1},
      ["electrons", "ions"]),
+    ("run_profile_channel.npz", {'window-length': 1.0, 'plasma-particles-per-cell': 9,
+                                 'plasma-rshape': 'channel', 'plasma-width': 0.6,
+                                 'plasma-width-2': 0.9, 'plasma-density-2': 0.5}, ["electrons"]),
+    ("run_profile_gauss.npz", {'window-length': 1.0, 'plasma-particles-per-cell': 1,
+                               'ion-model': 'mobile', 'plasma-rshape': 'gaussian',
+                               'plasma-width': 0.5}, ["electrons", "ions"]),
 ])
 def test_rigid_vs_reference(golden, fixture, extra, sorts):
     ref = golden(fixture)
