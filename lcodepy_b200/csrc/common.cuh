@@ -28,6 +28,22 @@ void count_launch(int n = 1);
 
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// One-time opt-in of a kernel to `bytes` of dynamic shared memory on the
+// current device; `done` remembers the devices already set (the attribute is
+// per device, so a process that uses several GPUs sets it on each).
+template <typename K>
+inline cudaError_t ensure_smem(K kernel, size_t bytes, unsigned long long &done)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = dev < 64 ? (1ull << dev) : 0ull;
+    if (bit && (done & bit)) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) done |= bit;
+    return e;
+}
+
 // ---- programmatic dependent launch ----
 // A kernel launched with launch_after() may be scheduled while its
 // predecessor in the stream is still running; it must call pdl_wait() before

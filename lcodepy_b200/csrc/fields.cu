@@ -1038,13 +1038,10 @@ static int launch_i8(const GemmBatch<T> &b, int nsub, int maxM, int maxN, cudaSt
     // one CTA per SM, read less operand data but ran no faster)
     constexpr int BN = Slices<T>::n == 8 ? 32 : 64;
     using Cfg = I8Cfg<Slices<T>::n, BN>;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_gemm_i8<T, BN, EPI>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)Cfg::smem);
+    static unsigned long long attr = 0;
+    {
+        const cudaError_t e = ensure_smem(k_gemm_i8<T, BN, EPI>, Cfg::smem, attr);
         if (e != cudaSuccess) return cuda_check(e, "i8 gemm smem attribute");
-        attr = true;
     }
     dim3 grid((maxN + BN - 1) / BN, (maxM + I8_BM - 1) / I8_BM, nsub);
     const cudaError_t e = launch_after(k_gemm_i8<T, BN, EPI>, grid, dim3(Cfg::THREADS), Cfg::smem, st, b);

@@ -989,12 +989,10 @@ static int launch_move_deposit_pair(const lcb_move_deposit_args *a, dim3 grid,
                                     typename StageAcc<FT>::type *const out[4], cudaStream_t st)
 {
     const size_t sm = move_deposit_pair_smem<FT, WX, WY>();
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_move_deposit_pair<FT, WX, WY, FIRST>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    static unsigned long long attr = 0;
+    {
+        const cudaError_t e = ensure_smem(k_move_deposit_pair<FT, WX, WY, FIRST>, sm, attr);
         if (e != cudaSuccess) return cuda_check(e, "move_deposit smem attribute");
-        attr = true;
     }
     const lcb_plasma_particles &p = a->prev, &f = a->full;
     const cudaError_t e = launch_after(
@@ -1113,13 +1111,9 @@ static int deposit_fixed(int64_t n_per_sort, int n_sorts, int N, double h, int p
         const dim3 grid((particles_side + DEP_TJ - 1) / DEP_TJ,
                         (particles_side + 1 + DEP_TI - 1) / DEP_TI, n_sorts);   // spare tile row
         const size_t sm = deposit_smem_bytes<fix_t>();
-        static bool attr = false;
-        if (!attr) {
-            e = cudaFuncSetAttribute(k_deposit_tiled<fix_t>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            if (e != cudaSuccess) return cuda_check(e, "deposit smem attribute");
-            attr = true;
-        }
+        static unsigned long long attr = 0;
+        e = ensure_smem(k_deposit_tiled<fix_t>, sm, attr);
+        if (e != cudaSuccess) return cuda_check(e, "deposit smem attribute");
         k_deposit_tiled<fix_t><<<grid, DEP_THREADS, sm, st>>>(
             n_per_sort, particles_side, N, h, x_init, y_init, x_offt, y_offt, px, py, pz, q, m,
             w, w + 2 * plane, w + 4 * plane, w + 6 * plane, err);
@@ -1209,13 +1203,9 @@ extern "C" int lcb_plasma_deposit(
                   (particles_side + 1 + DEP_TI - 1) / DEP_TI, n_sorts);   // spare tile row
         {
             const size_t sm = deposit_smem_bytes<double>();
-            static bool attr = false;
-            if (!attr) {
-                cudaError_t e = cudaFuncSetAttribute(k_deposit_tiled<double>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-                if (e != cudaSuccess) return cuda_check(e, "deposit smem attribute");
-                attr = true;
-            }
+            static unsigned long long attr = 0;
+            const cudaError_t e = ensure_smem(k_deposit_tiled<double>, sm, attr);
+            if (e != cudaSuccess) return cuda_check(e, "deposit smem attribute");
             k_deposit_tiled<double><<<grid, DEP_THREADS, sm, st>>>(
                 n_per_sort, particles_side, N, h, x_init, y_init, x_offt, y_offt,
                 px, py, pz, q, m, ro, jx, jy, jz, err);
