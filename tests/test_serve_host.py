@@ -1,5 +1,6 @@
 """Admission and retirement logic of the request server, with the GPU member
 replaced by a host fake (no device needed)."""
+import numpy as np
 import pytest
 
 torch = pytest.importorskip("torch")
@@ -116,3 +117,28 @@ def test_request_stream_mixes_rigid_and_beam_drivers():
             assert 100_000 <= drv.n <= 1_000_000
             half = cfg["window-width"] / 2
             assert drv.r_max < half
+
+
+def test_device_beam_distribution_on_cpu():
+    """The served drivers' beam generator (run here on CPU tensors): the
+    cuts, the charge normalisation and the moments of the bi-Gaussian."""
+    import math
+    drv = batch.BeamDriver(n=200_000, amplitude=0.3, sigma_r=0.8, sigma_z=1.0, xi0=-3.0,
+                           gamma=1000.0, espread=0.01, emittance=1e-2, seed=11, r_max=2.4)
+    b = drv.device_beam(0.05, torch.device("cpu"))
+    xi, x, y = b.xi.numpy(), b.x.numpy(), b.y.numpy()
+    n = xi.size
+    assert 0.95 * drv.n < n <= drv.n
+    assert (xi < 0).all() and (xi > 2 * drv.xi0).all()
+    assert (np.diff(xi) <= 0).all()                           # sorted, xi descending
+    r = np.hypot(x, y)
+    assert r.max() < drv.r_max
+    assert abs(np.std(b.pz.numpy()) / 1000.0 - 0.01) < 1e-3
+    assert abs(np.std(b.px.numpy()) - drv.emittance / drv.sigma_r) < 2e-4
+    q_total = (-drv.amplitude * math.sqrt(2 * math.pi) * drv.sigma_z
+               * 2 * math.pi * drv.sigma_r ** 2 / 0.05)
+    assert np.isclose(b.q_norm.numpy().sum(), q_total)
+    assert (b.q_m.numpy() == -1).all() and (np.sort(b.id.numpy()) == np.arange(1, n + 1)).all()
+    # seeded: the same driver gives the same beam
+    b2 = drv.device_beam(0.05, torch.device("cpu"))
+    assert np.array_equal(b2.x.numpy(), x)
