@@ -251,7 +251,6 @@ class FXiDiag(Diagnostic):
                 plt.savefig(self._directory / f'{name}_{current_time:08.2f}.jpg')
                 plt.close()
         self._data = defaultdict(list)
-        self._data['xi'] = []
         self._first = False
 
 
