@@ -416,9 +416,10 @@ def run_serve(args, ws, rank, local):
     clocks = clock.stop() if clock else None
     launches = _lib.launch_count() - n0
     ms = max_over_ranks(t0.elapsed_time(t1), ws)
-    done = srv.done
+    done = {r: d for r, d in srv.done.items() if "error" not in d}
+    failed = len(srv.done) - len(done)
     cell_steps = sum(d["cells"] * d["steps"] for d in done.values())
-    lat = np.array([done[r]["latency"] for _, r, _, _ in reqs])
+    lat = np.array([done[r]["latency"] for _, r, _, _ in reqs if r in done])
     value = ws * cell_steps / (ms / 1e3)
     # plain path, request by request, first come first served: per-step cost
     # per grid size, measured with a rigid driver and with a beam of the mean
@@ -430,6 +431,8 @@ def run_serve(args, ws, rank, local):
                 if any(isinstance(r[3], BeamDriver) for r in reqs) else per)
     finish, plain_lat, busy = 0.0, [], 0.0
     for arr, rid, cfg, drv in reqs:
+        if rid not in done:
+            continue
         d = done[rid]
         N = int(round(math.sqrt(d["cells"])))
         dur = d["steps"] * (per_beam if isinstance(drv, BeamDriver) else per)[N] / 1e3
@@ -442,15 +445,15 @@ def run_serve(args, ws, rank, local):
     errs = []
     if args.check_requests:
         from lcodepy_b200.batch import solo_ez
-        for arr, rid, cfg, drv in sorted(reqs, key=lambda r: r[2]['window-length'])[
-                :args.check_requests]:
+        for arr, rid, cfg, drv in sorted((r for r in reqs if r[1] in done),
+                                         key=lambda r: r[2]['window-length'])[:args.check_requests]:
             ez64 = solo_ez(cfg, drv, precision='fp64')
             errs.append(float(np.linalg.norm(done[rid]["ez"] - ez64) / np.linalg.norm(ez64)))
     return {"value": value, "ms": ms, "wall_s": wall, "cell_steps": cell_steps,
             "p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
             "plain_value": plain_value, "plain_p50": float(np.percentile(plain_lat, 50)),
             "plain_p99": float(np.percentile(plain_lat, 99)), "plain_ms_per_step": per,
-            "plain_ms_per_step_beam": per_beam,
+            "plain_ms_per_step_beam": per_beam, "failed": failed,
             "beam_requests": sum(isinstance(r[3], BeamDriver) for r in reqs),
             "errs": errs, "clocks": clocks, "launches": launches,
             "span_arrivals_s": reqs[-1][0]}
@@ -594,6 +597,7 @@ def main():
                            "steps_are": "requests; ms_per_step = makespan / requests",
                            "l2": "aggregate member state larger than L2"},
                 "latency_s": {"p50": r["p50"], "p99": r["p99"]},
+                "failed_requests": r["failed"],
                 "makespan_s": r["ms"] / 1e3, "cell_steps": r["cell_steps"],
                 "plain_fp64": {"value": r["plain_value"], "p50": r["plain_p50"],
                                "p99": r["plain_p99"],

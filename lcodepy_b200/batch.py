@@ -254,11 +254,15 @@ class Member:
         """All steps issued and executed."""
         return self.end_event is not None and self.end_event.query()
 
+    def check(self):
+        """Raise if a kernel of this member set a bit of a device error word."""
+        self.stream.synchronize()
+        self.solver.check_errors()
+
     def result(self):
         """On-axis Ez per xi step and the final fields (host arrays); raises if
         a kernel set a bit of the device error word."""
-        self.stream.synchronize()
-        self.solver.check_errors()
+        self.check()
         return {"ez": self.ez.cpu().numpy(),
                 "fields": self.solver.prev_fields.buf.cpu().numpy()}
 
@@ -323,12 +327,11 @@ class BeamMember(Member):
                 if self.done >= self.n_steps:
                     self.end_event = ev
 
-    def result(self):
-        out = super().result()
+    def check(self):
+        super().check()
         e = int(self.bc.err.item())
         if e:
             raise RuntimeError(f"beam device error word 0x{e:x} in member {self.name}")
-        return out
 
     def release(self):
         self.solver = None
@@ -457,7 +460,12 @@ class Server:
     its own stream), and ``retire`` collects requests whose last step has
     executed, releasing their memory so that waiting ones are admitted while
     others are still running.  Latency is measured from a request's arrival
-    to the moment its completion is observed."""
+    to the moment its completion is observed.
+
+    A request that cannot be set up (an invalid config, no device memory),
+    whose launches fail, or whose kernels set a bit of a device error word is
+    finished with ``done[id]["error"]`` (the exception text) and its memory is
+    released; the other requests carry on."""
 
     def __init__(self, hbm_budget_bytes: int, max_slots: int = 64, device=None):
         self.device = device or torch.device("cuda", torch.cuda.current_device())
@@ -481,6 +489,19 @@ class Server:
         else:
             self.waiting.append(item)
 
+    def _fail(self, rid, arrival, admitted, err: Exception):
+        t = self.now()
+        self.done[rid] = {"error": f"{type(err).__name__}: {err}", "ez": None,
+                          "latency": t - arrival, "arrival": arrival, "admitted": admitted,
+                          "finished": t}
+
+    def _drop(self, m, err: Exception):
+        self._fail(m.name, m.t_arrival, m.t_admit, err)
+        try:
+            m.release()
+        finally:
+            self.used -= m.footprint
+
     def poll(self):
         """Admit arrived requests, first come first served, while a slot is
         free and the footprint fits; a request that does not fit waits (and so
@@ -490,11 +511,20 @@ class Server:
             arr, rid, cfg, drv = self.waiting[0]
             if arr > t or len(self.running) + len(self.draining) >= self.max_slots:
                 break
-            fp = footprint_bytes(cfg, drv)
+            try:
+                fp = footprint_bytes(cfg, drv)
+            except Exception as e:      # an invalid config
+                self.waiting.popleft()
+                self._fail(rid, arr, None, e)
+                continue
             if self.used + fp > self.budget and (self.running or self.draining):
                 break
             self.waiting.popleft()
-            m = make_member(cfg, drv, self.device, name=rid)
+            try:
+                m = make_member(cfg, drv, self.device, name=rid)
+            except Exception as e:      # set-up failed (config, device memory)
+                self._fail(rid, arr, t, e)
+                continue
             m.t_arrival = arr
             m.t_admit = t
             m.footprint = fp
@@ -505,7 +535,11 @@ class Server:
         """One xi step for every running request."""
         keep = []
         for m in self.running:
-            m.step()
+            try:
+                m.step()
+            except Exception as e:      # a launch failed
+                self._drop(m, e)
+                continue
             (self.draining if m.finished else keep).append(m)
         self.running = keep
 
@@ -514,6 +548,11 @@ class Server:
         for m in self.draining:
             if m.complete():
                 t = self.now()
+                try:
+                    m.check()
+                except Exception as e:  # a device error word was set
+                    self._drop(m, e)
+                    continue
                 self.done[m.name] = {"ez": m.ez.cpu().numpy(), "latency": t - m.t_arrival,
                                      "arrival": m.t_arrival, "admitted": m.t_admit,
                                      "finished": t, "cells": m.cells, "steps": m.n_steps}

@@ -10,6 +10,9 @@ from lcodepy_b200 import batch  # noqa: E402
 
 class FakeMember:
     def __init__(self, cfg, drv, device=None, name=None):
+        if cfg.get("setup") == "fail":
+            raise MemoryError("no device memory")
+        self.fail_at = cfg.get("fail_at")
         self.name = name
         self.n_steps = cfg["steps"]
         self.cells = cfg["cells"]
@@ -21,14 +24,20 @@ class FakeMember:
         return self.done >= self.n_steps
 
     def step(self):
+        if self.fail_at is not None and self.done == self.fail_at:
+            raise RuntimeError("launch failed")
         self.ez[self.done] = self.done
         self.done += 1
 
     def complete(self):
         return self.finished
 
+    def check(self):
+        if self.cells == "device-error" and self.finished:
+            raise RuntimeError("device error word 0x1")
+
     def release(self):
-        pass
+        self.released = True
 
 
 @pytest.fixture
@@ -142,3 +151,20 @@ def test_device_beam_distribution_on_cpu():
     # seeded: the same driver gives the same beam
     b2 = drv.device_beam(0.05, torch.device("cpu"))
     assert np.array_equal(b2.x.numpy(), x)
+
+
+def test_failing_requests_are_isolated(fake):
+    srv = batch.Server(hbm_budget_bytes=100, max_slots=8, device="cpu")
+    srv.submit("ok", req(4, 10), None, arrival=0.0)
+    srv.submit("setup", {**req(4, 10), "setup": "fail"}, None, arrival=0.0)
+    srv.submit("launch", {**req(6, 10), "fail_at": 2}, None, arrival=0.0)
+    srv.submit("deverr", req(3, 10, cells="device-error"), None, arrival=0.0)
+    srv.submit("ok2", req(5, 10), None, arrival=0.0)
+    srv.run()
+    assert set(srv.done) == {"ok", "setup", "launch", "deverr", "ok2"}
+    assert "MemoryError" in srv.done["setup"]["error"]
+    assert "launch failed" in srv.done["launch"]["error"]
+    assert "device error" in srv.done["deverr"]["error"]
+    for rid in ("ok", "ok2"):
+        assert "error" not in srv.done[rid] and srv.done[rid]["ez"] is not None
+    assert srv.used == 0
