@@ -314,7 +314,7 @@ class BeamMember(Member):
         L = _lib.load()
         with torch.cuda.stream(self.stream):
             rb_full, rb_prev = bc.rho(i)
-            ps.step_dxi(rb_full, rb_prev, bc.rho_divisor)
+            ps.step_dxi(rb_full, rb_prev, bc.rho_divisor, stable_planes=True)
             bc.after_plasma_step(i, ps.last_fields, ps.prev_fields)
             _lib.check(L.lcb_record_axis(ps.prev_fields.Ez.data_ptr(), self.N,
                                          self.counter.data_ptr(), self.ez.data_ptr(),

@@ -66,7 +66,7 @@ class PusherAndSolver3D:
                 rb_full, rb_prev = bc.layout_beam_layer(None, xi_i)
             else:
                 rb_full, rb_prev = bc.rho(xi_i)
-            ps.step_dxi(rb_full, rb_prev, bc.rho_divisor)
+            ps.step_dxi(rb_full, rb_prev, bc.rho_divisor, stable_planes=not self.rigid)
             if not self.rigid:
                 # push layer i-1 between the previous and new fields, lay out i+1
                 bc.after_plasma_step(xi_i, ps.last_fields, ps.prev_fields)

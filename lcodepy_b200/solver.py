@@ -108,6 +108,7 @@ class Plane2d3vPlasmaSolver:
         self.graphs = [None, None]
         self.graph_launches = [0, 0]
         self.graph_div = None
+        self.plane_graphs = {}    # (parity, plane pointers, divisor) -> (graph, launches)
         self.eager_steps = 0
         # capture on the current (non-default) stream without the device-wide
         # synchronisation of torch.cuda.graph, for solvers that share the GPU
@@ -132,6 +133,9 @@ class Plane2d3vPlasmaSolver:
         dev = self.device
         if self.states is None or self.states[0].Ns != Ns:
             self.states = [PlasmaState(self.n_sorts, Ns, dev) for _ in range(2)]
+            # graphs captured on the previous particle buffers are stale
+            self.graphs = [None, None]
+            self.plane_graphs = {}
         st = self.states[0]
         n = Ns * Ns
         xi_t = torch.from_numpy(x_init.ravel()).to(dev)
@@ -280,45 +284,65 @@ class Plane2d3vPlasmaSolver:
     def prev_particles(self) -> PlasmaState:
         return self.states[self.cur]
 
-    def step_dxi(self, rb_full: torch.Tensor, rb_prev: torch.Tensor, rb_div: float = 1.0):
+    def step_dxi(self, rb_full: torch.Tensor, rb_prev: torch.Tensor, rb_div: float = 1.0,
+                 stable_planes: bool = False):
         """Advance the plasma by one xi step; afterwards the new state is the
         "prev" state (fields / currents / particles) and the step's input
         fields remain readable as ``last_fields`` until the next step.
 
         After two eager steps the step runs as a captured CUDA graph (one per
-        parity of the rotating buffers), unless per-op timing is requested."""
+        parity of the rotating buffers), unless per-op timing is requested.
+        The beam density planes are copied into fixed buffers that the graphs
+        read; with ``stable_planes`` (the caller rotates a few persistent
+        planes, as the non-rigid beam does) one graph per parity and plane
+        pair reads them in place instead."""
         if not self.use_graphs or self.op_timers is not None:
             self._step_ops(rb_full, rb_prev, rb_div)
             self.eager_steps += 1
             return
-        self.rbf.copy_(rb_full)
-        self.rbp.copy_(rb_prev)
-        if self.graph_div != rb_div:
-            self.graphs = [None, None]
-            self.graph_div = rb_div
         p = self.cur
-        if self.graphs[p] is None:
-            if self.eager_steps < 2:
-                self._step_ops(self.rbf, self.rbp, rb_div)
-                self.eager_steps += 1
-                return
-            g = torch.cuda.CUDAGraph()
-            n0 = _lib.load().lcb_launch_count()
-            if self.capture_on_stream:
-                g.capture_begin(capture_error_mode="thread_local")
-                try:
-                    self._step_ops(self.rbf, self.rbp, rb_div, advance=False)
-                finally:
-                    g.capture_end()
-            else:
-                with torch.cuda.graph(g):
-                    self._step_ops(self.rbf, self.rbp, rb_div, advance=False)
-            self.graph_launches[p] = _lib.load().lcb_launch_count() - n0
-            self.graphs[p] = g
-        self.graphs[p].replay()
-        _lib.add_replayed(self.graph_launches[p])
+        if stable_planes:
+            key = (p, rb_full.data_ptr(), rb_prev.data_ptr(), rb_div)
+            if key not in self.plane_graphs:
+                if self.eager_steps < 2:
+                    self._step_ops(rb_full, rb_prev, rb_div)
+                    self.eager_steps += 1
+                    return
+                self.plane_graphs[key] = self._capture(rb_full, rb_prev, rb_div)
+            g, nl = self.plane_graphs[key]
+        else:
+            self.rbf.copy_(rb_full)
+            self.rbp.copy_(rb_prev)
+            if self.graph_div != rb_div:
+                self.graphs = [None, None]
+                self.graph_div = rb_div
+            if self.graphs[p] is None:
+                if self.eager_steps < 2:
+                    self._step_ops(self.rbf, self.rbp, rb_div)
+                    self.eager_steps += 1
+                    return
+                self.graphs[p], self.graph_launches[p] = self._capture(self.rbf, self.rbp, rb_div)
+            g, nl = self.graphs[p], self.graph_launches[p]
+        g.replay()
+        _lib.add_replayed(nl)
         self.cur = 1 - p
         self.last_fields = self.fields[p]
+
+    def _capture(self, rb_full, rb_prev, rb_div):
+        """Capture one xi step (for the current buffer parity) reading the
+        given beam density planes; returns (graph, launches in it)."""
+        g = torch.cuda.CUDAGraph()
+        n0 = _lib.load().lcb_launch_count()
+        if self.capture_on_stream:
+            g.capture_begin(capture_error_mode="thread_local")
+            try:
+                self._step_ops(rb_full, rb_prev, rb_div, advance=False)
+            finally:
+                g.capture_end()
+        else:
+            with torch.cuda.graph(g):
+                self._step_ops(rb_full, rb_prev, rb_div, advance=False)
+        return g, _lib.load().lcb_launch_count() - n0
 
     def _step_ops(self, rb_full, rb_prev, rb_div, advance=True):
         p, f = self.cur, 1 - self.cur
