@@ -15,15 +15,21 @@ inputs live in HBM and exceed L2 (plasma state 134 MB, beam 88 MB), so no
 extra L2 flush is done.  With --gpus N (torchrun) every rank runs its own
 replica (the xi loop does not shard): weak scaling.
 
+The default line also carries the many-simulation forms (at one GPU):
+"batched" -- the 64-member scan in mixed precision against the same members
+run one by one through the plain FP64 drop-in path -- and "served" -- the
+request stream in mixed precision against the same requests run one by one,
+first come first served, through the plain FP64 path (each timed for real).
+
 --impl reference times the CPU restatement of the reference algorithm
-(oracle/, the reference's own numba path cannot be shipped here) on the
-host cores, on a bounded prefix of the same xi loop.
+(oracle/: the reference's Python package cannot travel with this tree) on
+the host cores, on a bounded sample of the same xi loop.
 """
 from __future__ import annotations
 
 import argparse
+import contextlib
 import json
-import math
 import os
 import subprocess
 import sys
@@ -208,7 +214,10 @@ def run_gpu(args, ws, rank, local):
     # ---- end to end through the public API, host buffers in and out ----
     e2e = None if args.no_e2e else run_e2e(cfg, beam_host, dev)
 
-    return dict(value=value, ms_per_step=ms_per_step, N=N, ops=ops,
+    Ns = ps.plasma_solver.states[0].Ns
+    n_particles = Ns * Ns * (2 if conf.get('ion-model') == 'mobile' else 1)
+    del source, drain, sim, ps
+    return dict(value=value, ms_per_step=ms_per_step, N=N, ops=ops, n_particles=n_particles,
                 launches=int(ev["l1"] - ev["l0"]), clocks=ev.get("clocks"),
                 e2e=e2e, n_iter=n_iter)
 
@@ -307,7 +316,8 @@ def run_batch(args, ws, rank, local):
     del members, runner
     torch.cuda.empty_cache()
 
-    # plain FP64: each member alone, eager, no graphs, separate kernels
+    # plain FP64: each member alone through the drop-in path with its default
+    # settings (captured graphs, fused particle stage): the fastest FP64 form
     plain_ms, errs = 0.0, []
     for (cfg, drv), ezb in zip(specs, ez_batch):
         c = {**cfg, 'precision': 'fp64'}
@@ -336,40 +346,41 @@ def run_batch(args, ws, rank, local):
             "clocks": clocks, "cells": cells, "members": len(specs), "launches": launches}
 
 
-def plain_ms_per_step(N, precision="fp64", n_steps=120, skip=20, beam=None):
-    """Device ms per xi step of the plain drop-in path (PusherAndSolver3D
-    with default settings) on an N x N grid at h = dxi = 0.05, with a rigid
-    Gaussian driver or the given BeamDriver."""
+def run_plain_requests(reqs, dev):
+    """Run each (arrival, id, config, driver) request alone through the
+    drop-in Simulation API in FP64; returns {id: {seconds, ez}}.  A beam
+    driver's particle file is written before its clock starts (the served
+    path generates beams on the device in milliseconds)."""
     import torch
-    from lcodepy_b200.batch import GaussianDriver, request_stream
-    from lcodepy_b200.beam3d import BeamDrain, BeamSource, RigidBeamSource
-    from lcodepy_b200.config import Config
-    from lcodepy_b200.push_solver import PusherAndSolver3D
-    cfg = dict(request_stream(n=1, sizes=(N,), min_steps=n_steps, max_steps=n_steps,
-                              beam_fraction=0.0)[0][2])
-    cfg['precision'] = precision
-    cfg['rigid-beam'] = beam is None
-    conf = Config(cfg)
-    conf._adjust_config_values_3d()
-    dev = torch.device("cuda", torch.cuda.current_device())
-    ps = PusherAndSolver3D(conf, dev)
-    ev = {}
-
-    def hook(k):
-        if k in (skip, n_steps):
-            ev[k] = torch.cuda.Event(enable_timing=True)
-            ev[k].record()
-    ps.plasma_solver.init_state(1.0)
-    if beam is None:
-        src, drain = RigidBeamSource(None, GaussianDriver()), None
-    else:
-        import dataclasses
-        beam = dataclasses.replace(beam, r_max=min(beam.r_max, 0.4 * cfg['window-width']))
-        src = BeamSource(conf, beam.device_beam(cfg['xi-step'], dev), dev)
-        drain = BeamDrain(conf, dev)
-    ps.step_dt(cfg['xi-step'], src, drain, 1.0, [], step_hook=hook)
-    torch.cuda.synchronize()
-    return ev[skip].elapsed_time(ev[n_steps]) / (n_steps - skip)
+    from lcodepy_b200 import Simulation
+    from lcodepy_b200.batch import BeamDriver
+    out = {}
+    with tempfile.TemporaryDirectory() as td:
+        for arr, rid, cfg, drv in reqs:
+            c = {**cfg, 'precision': 'fp64'}
+            path = None
+            if isinstance(drv, BeamDriver):
+                c['rigid-beam'] = False
+                c.setdefault('time-limit', 1.0)
+                beam = drv.particles(float(c['xi-step']))
+                path = os.path.join(td, "beam.npz")
+                np.savez(path, **{k: beam[k] for k in beam.dtype.names})
+                del beam
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            with contextlib.redirect_stdout(sys.stderr):   # Simulation's progress notes
+                if path is None:
+                    sim = Simulation(config=c, beam_parameters=drv, runas_filename='')
+                    sim.step()
+                else:
+                    sim = Simulation(config=c, runas_filename='')
+                    sim.load_beamfile(path)
+                    sim.step(1)
+            ez = sim.push_solver.ez_axis.cpu().numpy()
+            torch.cuda.synchronize()
+            out[rid] = {"seconds": time.perf_counter() - t0, "ez": ez}
+            del sim
+    return out
 
 
 def run_serve(args, ws, rank, local):
@@ -379,9 +390,9 @@ def run_serve(args, ws, rank, local):
     bi-Gaussian beams of 100k..1M macroparticles; admitted by HBM footprint into at
     most --slots concurrent members, each advanced by captured graphs on its
     own stream.  The plain comparison runs the same requests one by one, first
-    come first served, through the plain FP64 drop-in path; its per-step cost
-    per grid size is measured here and its schedule computed from the
-    arrivals."""
+    come first served, through the plain FP64 drop-in path (Simulation with
+    its default settings), each timed for real; its queue follows from the
+    arrivals and the measured durations."""
     import torch
     from lcodepy_b200 import _lib
     from lcodepy_b200.batch import Server, request_stream
@@ -421,39 +432,30 @@ def run_serve(args, ws, rank, local):
     cell_steps = sum(d["cells"] * d["steps"] for d in done.values())
     lat = np.array([done[r]["latency"] for _, r, _, _ in reqs if r in done])
     value = ws * cell_steps / (ms / 1e3)
-    # plain path, request by request, first come first served: per-step cost
-    # per grid size, measured with a rigid driver and with a beam of the mean
-    # size (550k macroparticles)
-    from lcodepy_b200.batch import BeamDriver
-    per = {N: plain_ms_per_step(N) for N in (129, 257, 513)}
-    per_beam = ({N: plain_ms_per_step(N, beam=BeamDriver(n=550_000, amplitude=0.1))
-                 for N in (129, 257, 513)}
-                if any(isinstance(r[3], BeamDriver) for r in reqs) else per)
-    finish, plain_lat, busy = 0.0, [], 0.0
-    for arr, rid, cfg, drv in reqs:
-        if rid not in done:
+    # plain path, request by request, first come first served: every request
+    # runs alone through the drop-in Simulation API in FP64 (its defaults:
+    # graphs and the fused particle stage), timed by wall clock from
+    # construction to the synchronised end of its xi loop.  One request runs
+    # at a time, so the queue is exact from the measured durations: request i
+    # starts at max(arrival_i, end of request i-1).
+    plain = run_plain_requests([r for r in reqs if r[1] in done], dev)
+    finish, plain_lat = 0.0, []
+    for arr, rid, _, _ in reqs:
+        if rid not in plain:
             continue
-        d = done[rid]
-        N = int(round(math.sqrt(d["cells"])))
-        dur = d["steps"] * (per_beam if isinstance(drv, BeamDriver) else per)[N] / 1e3
-        finish = max(finish, arr) + dur
-        busy += dur
+        finish = max(finish, arr) + plain[rid]["seconds"]
         plain_lat.append(finish - arr)
     plain_lat = np.array(plain_lat)
     plain_value = cell_steps / finish
     # accuracy: a few requests rerun alone through the plain FP64 path
-    errs = []
-    if args.check_requests:
-        from lcodepy_b200.batch import solo_ez
-        for arr, rid, cfg, drv in sorted((r for r in reqs if r[1] in done),
-                                         key=lambda r: r[2]['window-length'])[:args.check_requests]:
-            ez64 = solo_ez(cfg, drv, precision='fp64')
-            errs.append(float(np.linalg.norm(done[rid]["ez"] - ez64) / np.linalg.norm(ez64)))
+    # accuracy: every served result against the same request alone in FP64
+    errs = [float(np.linalg.norm(done[rid]["ez"] - plain[rid]["ez"]) /
+                  max(np.linalg.norm(plain[rid]["ez"]), 1e-300)) for rid in plain]
     return {"value": value, "ms": ms, "wall_s": wall, "cell_steps": cell_steps,
             "p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
             "plain_value": plain_value, "plain_p50": float(np.percentile(plain_lat, 50)),
-            "plain_p99": float(np.percentile(plain_lat, 99)), "plain_ms_per_step": per,
-            "plain_ms_per_step_beam": per_beam, "failed": failed,
+            "plain_p99": float(np.percentile(plain_lat, 99)),
+            "plain_busy_s": sum(v["seconds"] for v in plain.values()), "failed": failed,
             "beam_requests": sum(isinstance(r[3], BeamDriver) for r in reqs),
             "errs": errs, "clocks": clocks, "launches": launches,
             "span_arrivals_s": reqs[-1][0]}
@@ -493,18 +495,81 @@ def run_e2e(cfg, beam_host, dev):
 # CPU arm (oracle restatement of the reference algorithm)
 # ---------------------------------------------------------------------------
 
-def run_cpu_sample(xi_steps_sample, beam_host):
-    """The oracle on the host cores for the first `xi_steps_sample` xi steps of
-    the workload; returns (xi-steps*cells/s, seconds, threads)."""
+def run_headline(args, ws, rank, local):
+    """The many-simulation forms carried by the default line: the batched
+    scan (64 members, mixed precision, 30 timed batched xi steps) and the
+    served stream (`--requests` requests, mixed precision), each against the
+    plain FP64 drop-in path run member by member / request by request."""
+    import torch
+    out = {}
+    torch.cuda.empty_cache()
+    bargs = argparse.Namespace(**{**vars(args), "steps": 30, "warmup": 3, "precision": "mixed"})
+    try:
+        b = run_batch(bargs, ws, rank, local)
+        out["batched"] = {
+            "workload": f"batched scan: {b['members']} members, grids 129/257/513 at h=0.05, "
+                        "dxi=0.05, ppc=4, seeded rigid Gaussian drivers; 30 timed batched xi "
+                        "steps after 3",
+            "precision": "mixed", "value": b["value"], "unit": METRIC,
+            "ms_per_batched_step": b["ms_per_step"], "plain_fp64_value": b["plain"],
+            "batched_vs_plain": b["ratio"],
+            "ez_rel_l2_vs_fp64": {"max": b["ez_err_max"], "median": b["ez_err_median"]},
+            "gpu_launches": b["launches"], "clocks": b["clocks"]}
+    except Exception as e:  # reported, not fatal to the production line
+        out["batched"] = {"error": f"{type(e).__name__}: {e}"}
+    torch.cuda.empty_cache()
+    sargs = argparse.Namespace(**{**vars(args), "precision": "mixed"})
+    try:
+        v = run_serve(sargs, ws, rank, local)
+        out["served"] = {
+            "workload": f"served stream: {args.requests} requests (Poisson 20/s, seeded), grids "
+                        "129/257/513 at h=0.05, 200-2000 xi steps of 0.05, half rigid "
+                        "Gaussian, half bi-Gaussian beams of 100k-1M macroparticles",
+            "precision": "mixed", "value": v["value"], "unit": METRIC,
+            "latency_s": {"p50": v["p50"], "p99": v["p99"]},
+            "plain_fp64": {"value": v["plain_value"], "p50": v["plain_p50"],
+                           "p99": v["plain_p99"], "busy_s": v["plain_busy_s"],
+                           "how": "each request alone through Simulation, timed; FCFS queue "
+                                  "from the arrivals and the measured durations"},
+            "served_vs_plain": v["value"] / v["plain_value"],
+            "ez_rel_l2_vs_fp64": {"max": max(v["errs"]) if v["errs"] else None,
+                                  "median": float(np.median(v["errs"])) if v["errs"] else None},
+            "failed_requests": v["failed"], "gpu_launches": v["launches"],
+            "clocks": v["clocks"]}
+    except Exception as e:
+        out["served"] = {"error": f"{type(e).__name__}: {e}"}
+    return out
+
+
+class _Budget(Exception):
+    pass
+
+
+def run_cpu_sample(warmup, steps, beam_host, budget_s=90.0):
+    """The oracle on the host cores over the workload's xi loop: `warmup` xi
+    steps untimed, then up to `steps` timed xi steps, stopping early once
+    `budget_s` seconds of timed work are done.  Returns (xi-steps*cells/s,
+    seconds, timed steps, threads)."""
     from oracle import oracle as O
     p = O.make_params(5.13, 0.02, 0.02)
     sorts, consts = O.init_plasma(p)
     F, cur = O.Fields.zeros(p.N), O.Currents.zeros(p.N)
     beam = O.Beam.from_array(beam_host).sorted()
-    t0 = time.perf_counter()
-    O.step_dt(p, sorts, F, cur, consts, xi_steps_sample - 1, beam=beam, time_step=1.0)
-    dt = time.perf_counter() - t0
-    return xi_steps_sample * p.N * p.N / dt, dt, O.num_threads()
+    stamps = []
+
+    def record(i, *_):
+        stamps.append(time.perf_counter())
+        timed = len(stamps) - 1 - warmup
+        if timed >= steps or (timed > 0 and stamps[-1] - stamps[warmup] > budget_s):
+            raise _Budget
+    try:
+        O.step_dt(p, sorts, F, cur, consts, warmup + steps, beam=beam, time_step=1.0,
+                  record=record)
+    except _Budget:
+        pass
+    n = len(stamps) - 1 - warmup
+    dt = stamps[-1] - stamps[warmup]
+    return n * p.N * p.N / dt, dt, n, O.num_threads()
 
 
 def main():
@@ -518,14 +583,17 @@ def main():
     ap.add_argument("--requests", type=int, default=64, help="serve: requests in the stream")
     ap.add_argument("--slots", type=int, default=32, help="serve: concurrent members")
     ap.add_argument("--hbm-budget-gb", type=int, default=64, help="serve: HBM admission budget")
-    ap.add_argument("--check-requests", type=int, default=3,
-                    help="serve: requests rerun alone in FP64 for the Ez error")
     ap.add_argument("--workload", default="production",
                     choices=["production", "rigid129", "batch", "serve"],
                     help="production: the N=513 FP64 drop-in run (default); rigid129: "
                          "the 129 x 129 rigid-driver configuration")
     ap.add_argument("--cpu-sample", type=int, default=8,
-                    help="xi steps of the CPU baseline sample")
+                    help="timed xi steps of the CPU baseline sample")
+    ap.add_argument("--cpu-budget", type=float, default=90.0,
+                    help="reference arm: seconds of timed CPU work at most")
+    ap.add_argument("--no-headline", action="store_true",
+                    help="production line only: skip the batched scan and the served "
+                         "stream that the default line carries")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the end-to-end Simulation run (profiling runs)")
@@ -539,18 +607,20 @@ def main():
 
     if args.impl == "reference":
         if rank == 0:
-            beam = make_beam()
-            n = max(2, min(args.steps, args.cpu_sample))
-            v, dt, thr = run_cpu_sample(n, beam)
+            W = min(args.warmup, 3)
+            v, dt, n, thr = run_cpu_sample(W, args.steps, make_beam(), args.cpu_budget)
             line = {"metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
-                    "steps": n, "warmup": 0, "ms_per_step": dt * 1e3 / n,
+                    "steps": n, "warmup": W, "ms_per_step": dt * 1e3 / n,
                     "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                    "dtype": "f64", "data": "synthetic", "impl": "reference",
+                    "dtype": "f64", "data": "synthetic (seeded bi-Gaussian beam, uniform plasma)",
+                    "impl": "reference",
                     "config": {"workload": WORKLOAD, "parallelism": "replicas",
                                "l2": "inputs larger than L2"},
                     "cpu_baseline": {"value": v, "unit": METRIC, "cores": thr, "kind": "port",
-                                     "sample": f"first {n} xi steps of the workload "
-                                               "(oracle/: C particle loops + scipy DST/DCT)"},
+                                     "sample": f"xi steps {W + 1}..{W + n} of the workload "
+                                               f"({dt:.1f} s; the oracle's C particle loops "
+                                               f"with OpenMP + scipy DST/DCT; at most "
+                                               f"{args.cpu_budget:g} s of timed work)"},
                     "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0,
                             "d2h_bytes_per_step": 0}}
             print(json.dumps(line), flush=True)
@@ -600,11 +670,10 @@ def main():
                 "failed_requests": r["failed"],
                 "makespan_s": r["ms"] / 1e3, "cell_steps": r["cell_steps"],
                 "plain_fp64": {"value": r["plain_value"], "p50": r["plain_p50"],
-                               "p99": r["plain_p99"],
-                               "ms_per_step": r["plain_ms_per_step"],
-                               "ms_per_step_beam": r["plain_ms_per_step_beam"]},
+                               "p99": r["plain_p99"], "busy_s": r["plain_busy_s"]},
                 "served_vs_plain": r["value"] / r["plain_value"],
-                "ez_rel_l2_vs_fp64": r["errs"],
+                "ez_rel_l2_vs_fp64": {"max": max(r["errs"]) if r["errs"] else None,
+                                      "median": float(np.median(r["errs"])) if r["errs"] else None},
                 "gpu_launches": r["launches"], "clocks": r["clocks"]}), flush=True)
         return
     if args.workload == "rigid129":
@@ -623,6 +692,9 @@ def main():
                   flush=True)
         return
     r = run_gpu(args, ws, rank, local)
+    headline = {}
+    if not args.no_headline and ws == 1:
+        headline = run_headline(args, ws, rank, local)
     if rank == 0:
         N = r["N"]
         peaks = {}
@@ -630,16 +702,14 @@ def main():
             peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         except (OSError, ValueError):
             pass
-        hbm_peak = peaks.get("hbm_gbs", 6650.0)
-        peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
         r["precision"] = args.precision
-        roof = roofline(r, N, hbm_peak, peak_src, peaks)
+        roof = roofline(r, N, peaks)
         cpu = None
         if not args.no_cpu_baseline:
-            v, dt, thr = run_cpu_sample(args.cpu_sample, make_beam())
+            v, dt, n, thr = run_cpu_sample(1, args.cpu_sample, make_beam(), 30.0)
             cpu = {"value": v, "unit": METRIC, "cores": thr, "kind": "port",
-                   "sample": f"first {args.cpu_sample} xi steps of the workload on the host "
-                             f"({dt:.1f} s; oracle/: C particle loops, scipy DST/DCT)"}
+                   "sample": f"xi steps 2..{n + 1} of the workload on the host ({dt:.1f} s; "
+                             "the oracle's C particle loops with OpenMP + scipy DST/DCT)"}
         line = {"metric": METRIC, "value": r["value"], "unit": METRIC, "n_gpus": ws,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -657,61 +727,63 @@ def main():
                 "roofline": roof, "cpu_baseline": cpu,
                 "ops": {k: {"launches": v["launches"], "ms_avg": round(v["ms_avg"], 5),
                             "ms_total": round(v["ms_total"], 2)} for k, v in r["ops"].items()}}
+        line.update(headline)
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
 
 
-# DRAM bytes (read + written) per call of the dominant op, from one ncu
-# capture of the small case of the same workload (N=513, 11 xi steps):
-# compute_fields counts its four tensor-core waves, move_deposit the fused
-# kernel of a non-first stage.
-NCU_TRAFFIC = {("compute_fields", "fp64"): 85.1e6, ("compute_fields", "mixed"): 43.8e6,
-               ("move_deposit", "fp64"): 118.2e6, ("move_deposit", "mixed"): 115.5e6}
+# DRAM bytes (read + written) per call of each op, summed over all of the
+# op's kernels, from one ncu capture of the small case of the same workload
+# (N=513, window 0.2: 11 xi steps; profiles/launches_production_n513.md).
+NCU_TRAFFIC = {("compute_fields", "fp64"): None, ("compute_fields", "mixed"): None,
+               ("move_deposit", "fp64"): None, ("move_deposit", "mixed"): None}
+
+# algorithmic bytes per plasma particle and xi step: K1 64 B (read m, px, py,
+# pz, x_offt, y_offt; write x_offt, y_offt) + 3 x K2 128 B (read 11 x 8 B,
+# write 5 x 8 B) + 3 x K3 72 B (read 9 x 8 B) = 664 B, over the xi step's
+# three fused stages (K1 runs in the first): 664 / 3 B per stage on average
+STAGE_BYTES = 664.0 / 3
 
 
-def transform_flops(N):
-    """Flops of the dense transforms of one compute_fields call: four waves
-    of even/odd folded products (2 M K N each) over the seven problems, Phi
-    counted in one call of two (the predictor does not need it)."""
-    n = N - 2
-    rows = [n, n, N, N, n, n, N]
-    cols = [N, N, n, n, n, n, N]
-    tot = 0.0
-    for p in range(7):
-        R, C = rows[p], cols[p]
-        right = 2 * R * (((C + 1) // 2) ** 2 + ((C - 1) // 2) ** 2)
-        left = 2 * C * (((R + 1) // 2) ** 2 + ((R - 1) // 2) ** 2)
-        tot += (0.5 if p == 5 else 1.0) * 2 * (right + left)
-    return tot
+def op_roofline(name, o, N, Np, precision, peaks):
+    """Roofline of one op from its per-call CUDA-event time `o["ms_avg"]`:
+    compute_fields against the measured bf16 burst peak with the useful
+    dense-transform flops 56 N^3 per call (two calls per xi step make the
+    112 N^3 per xi step of the transforms as dense contractions), the fused
+    particle stage against the measured HBM copy bandwidth with 664 / 3 B
+    per particle (the xi step's 664 B over its three stages)."""
+    sec = o["ms_avg"] / 1e3
+    if name == "compute_fields":
+        peak = peaks.get("bf16_tflops")
+        flops = 56.0 * N ** 3
+        achieved = flops / sec / 1e12
+        return {"bound": "tensor", "kernel": name, "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+                "work_per_launch": f"{flops:.4g} flop (56 N^3, N={N})",
+                "traffic": NCU_TRAFFIC.get((name, precision)),
+                "peak_source": "measured bf16 burst" if peak else "absent"}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    nbytes = STAGE_BYTES * Np
+    achieved = nbytes / sec / 1e9
+    return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
+            "unit": "GB/s", "frac": achieved / peak,
+            "work_per_launch": f"{nbytes:.4g} B (664/3 B x {Np} particles)",
+            "traffic": NCU_TRAFFIC.get((name, precision)),
+            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback 6650 GB/s"}
 
 
-def roofline(r, N, hbm_peak, peak_src, peaks):
-    """Roofline of the dominant operation over the timed region."""
-    ops = r["ops"]
+def roofline(r, N, peaks):
+    """The dominant op's roofline (largest device time in the timed region),
+    with every measured op's roofline under "ops"."""
+    ops = {k: v for k, v in r["ops"].items() if k in ("compute_fields", "move_deposit")}
     if not ops:
         return None
+    Np = r["n_particles"]
+    each = {k: op_roofline(k, v, N, Np, r["precision"], peaks) for k, v in ops.items()}
     name = max(ops, key=lambda k: ops[k]["ms_total"])
-    o = ops[name]
-    Np = 964 * 964
-    if name == "compute_fields":
-        # executed int8 operations: one slice-pair product per pair i + j < NS
-        prec = r.get("precision", "fp64")
-        ns = 8 if prec == "fp64" else 4
-        ops_int8 = ns * (ns + 1) // 2 * transform_flops(N)
-        achieved = ops_int8 / (o["ms_avg"] / 1e3) / 1e12
-        return {"bound": "tensor", "kernel": name + f" (int8 tcgen05 waves, {ns} slices)",
-                "achieved": achieved, "peak": 4500.0, "unit": "TOP/s", "frac": achieved / 4500.0,
-                "traffic": NCU_TRAFFIC.get((name, prec)),
-                "peak_source": "nominal B200 dense int8 (no measured int8 peak on this pool)"}
-    per = {"deposit": 72, "move_smart": 128, "move_wo_fields": 64,
-           "move_deposit": 128 + 72}.get(name, 0)
-    achieved = per * Np / (o["ms_avg"] / 1e3) / 1e9
-    return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm_peak,
-            "unit": "GB/s", "frac": achieved / hbm_peak,
-            "traffic": NCU_TRAFFIC.get((name, r.get("precision", "fp64"))),
-            "peak_source": peak_src}
+    return {**each[name], "ops": each}
 
 
 if __name__ == "__main__":

@@ -286,7 +286,7 @@ typedef struct lcb_beam_step_args {
  * deposit only reads the source, so a caller may lay out layer i+1 right
  * after the plasma step of layer i.  Replaces the per-layer
  * body of PusherAndSolver3D.step_dt for a non-rigid beam,
- * lcode/push_solvers/push_solver.py:506-531 (layout_beam_layer,
+ * lcode/push_solvers/push_solver.py:237-261 (layout_beam_layer,
  * move_beam_layer, create_next_layer, push_beam_layer). */
 int lcb_beam_step(const lcb_beam_step_args *a, void *stream);
 
@@ -309,7 +309,7 @@ int lcb_rigid_gaussian(int grid_steps, double h, double xi_step, double amplitud
 
 /* history[*counter] = plane[N/2][N/2] (the on-axis value), then *counter += 1.
  * The device-side form of the per-step on-axis Ez record
- * (push_solver.py:541-547). */
+ * (push_solver.py:272-278). */
 int lcb_record_axis(const double *plane, int grid_steps, int64_t *counter,
                     double *history, int64_t capacity, void *stream);
 

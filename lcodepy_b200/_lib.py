@@ -15,6 +15,8 @@ LIB_PATH = os.path.join(HERE, "liblcb.so")
 LCB_OK = 0
 LCB_PREC_FP64 = 0
 LCB_PREC_MIXED = 1
+# size of the fixed device scratch array of lcb_compute_fields_noalloc (lcb.h)
+LCB_NOALLOC_FIELDS_SCRATCH_BYTES = 16 << 20
 DEVERR_PLASMA_STENCIL = 1
 DEVERR_BEAM_STENCIL = 2
 DEVERR_CAPACITY = 4

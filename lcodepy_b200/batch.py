@@ -497,6 +497,13 @@ class Server:
 
     def _drop(self, m, err: Exception):
         self._fail(m.name, m.t_arrival, m.t_admit, err)
+        # work queued earlier on the member's stream may still read or write
+        # its buffers: wait for it before they go back to the allocator (a
+        # stream in an error state raises again; its work is over then)
+        try:
+            m.stream.synchronize()
+        except Exception:
+            pass
         try:
             m.release()
         finally:

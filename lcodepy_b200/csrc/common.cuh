@@ -5,6 +5,8 @@
 #include <stdint.h>
 #include <stdio.h>
 
+#include <atomic>
+
 #include "../../include/lcb.h"
 
 namespace lcb {
@@ -30,17 +32,19 @@ inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s
 
 // One-time opt-in of a kernel to `bytes` of dynamic shared memory on the
 // current device; `done` remembers the devices already set (the attribute is
-// per device, so a process that uses several GPUs sets it on each).
+// per device, so a process that uses several GPUs sets it on each).  Host
+// threads driving different GPUs may call this at once: the mask is atomic,
+// and setting the attribute twice for one device is harmless.
 template <typename K>
-inline cudaError_t ensure_smem(K kernel, size_t bytes, unsigned long long &done)
+inline cudaError_t ensure_smem(K kernel, size_t bytes, std::atomic<unsigned long long> &done)
 {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     const unsigned long long bit = dev < 64 ? (1ull << dev) : 0ull;
-    if (bit && (done & bit)) return cudaSuccess;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
     e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e == cudaSuccess) done |= bit;
+    if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_acq_rel);
     return e;
 }
 

@@ -1038,7 +1038,7 @@ static int launch_i8(const GemmBatch<T> &b, int nsub, int maxM, int maxN, cudaSt
     // one CTA per SM, read less operand data but ran no faster)
     constexpr int BN = Slices<T>::n == 8 ? 32 : 64;
     using Cfg = I8Cfg<Slices<T>::n, BN>;
-    static unsigned long long attr = 0;
+    static std::atomic<unsigned long long> attr{0};
     {
         const cudaError_t e = ensure_smem(k_gemm_i8<T, BN, EPI>, Cfg::smem, attr);
         if (e != cudaSuccess) return cuda_check(e, "i8 gemm smem attribute");

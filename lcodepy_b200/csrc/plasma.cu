@@ -989,7 +989,7 @@ static int launch_move_deposit_pair(const lcb_move_deposit_args *a, dim3 grid,
                                     typename StageAcc<FT>::type *const out[4], cudaStream_t st)
 {
     const size_t sm = move_deposit_pair_smem<FT, WX, WY>();
-    static unsigned long long attr = 0;
+    static std::atomic<unsigned long long> attr{0};
     {
         const cudaError_t e = ensure_smem(k_move_deposit_pair<FT, WX, WY, FIRST>, sm, attr);
         if (e != cudaSuccess) return cuda_check(e, "move_deposit smem attribute");
@@ -1111,7 +1111,7 @@ static int deposit_fixed(int64_t n_per_sort, int n_sorts, int N, double h, int p
         const dim3 grid((particles_side + DEP_TJ - 1) / DEP_TJ,
                         (particles_side + 1 + DEP_TI - 1) / DEP_TI, n_sorts);   // spare tile row
         const size_t sm = deposit_smem_bytes<fix_t>();
-        static unsigned long long attr = 0;
+        static std::atomic<unsigned long long> attr{0};
         e = ensure_smem(k_deposit_tiled<fix_t>, sm, attr);
         if (e != cudaSuccess) return cuda_check(e, "deposit smem attribute");
         k_deposit_tiled<fix_t><<<grid, DEP_THREADS, sm, st>>>(
@@ -1203,7 +1203,7 @@ extern "C" int lcb_plasma_deposit(
                   (particles_side + 1 + DEP_TI - 1) / DEP_TI, n_sorts);   // spare tile row
         {
             const size_t sm = deposit_smem_bytes<double>();
-            static unsigned long long attr = 0;
+            static std::atomic<unsigned long long> attr{0};
             const cudaError_t e = ensure_smem(k_deposit_tiled<double>, sm, attr);
             if (e != cudaSuccess) return cuda_check(e, "deposit smem attribute");
             k_deposit_tiled<double><<<grid, DEP_THREADS, sm, st>>>(

@@ -1,4 +1,4 @@
-"""The xi loop of one time step (lcode/push_solvers/push_solver.py:458-555).
+"""The xi loop of one time step (lcode/push_solvers/push_solver.py:215-286).
 
 Per xi step i = 0 .. round(window-length / xi-step) (inclusive, as in the
 reference):

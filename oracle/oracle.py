@@ -475,7 +475,7 @@ def layer_length(beam: Beam, head: int, layer_idx: int, dxi: float) -> int:
 
 
 # --------------------------------------------------------------------------
-# xi loop (push_solvers/push_solver.py:484-555)
+# xi loop (push_solvers/push_solver.py:215-286)
 # --------------------------------------------------------------------------
 
 def step_dt(p: Params, sorts, F: Fields, cur: Currents, consts: Consts,

@@ -8,7 +8,11 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-REFERENCE_DATA = "/root/reference/tests/integration/data"
+# the reference checkout's own golden data (read only where it is present);
+# the checkout is located by the oracle's recipe (LCODE_REFERENCE)
+from oracle.ref_kernels import reference_root  # noqa: E402
+
+REFERENCE_DATA = os.path.join(reference_root(), "tests", "integration", "data")
 
 
 def pytest_configure(config):

@@ -277,4 +277,6 @@ def make_test1(lcode):
 
 if __name__ == '__main__':
     args = [a for a in sys.argv[1:] if not a.startswith('--')]
-    main(args[0] if args else '/root/reference')
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from oracle.ref_kernels import reference_root
+    main(args[0] if args else reference_root())

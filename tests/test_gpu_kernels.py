@@ -219,9 +219,13 @@ def test_compute_fields(golden, precision, rel):
         close(N_(outs[1][i]), d["half_" + k], rel, "half " + k)
 
 
-@pytest.mark.parametrize("N", [33, 129, 257])
-def test_compute_fields_sizes_vs_oracle(N):
-    """Random smooth currents at several grid sizes (both GEMM tilings)."""
+@pytest.mark.parametrize("precision,rel", [(_lib.LCB_PREC_FP64, 1e-11),
+                                           (_lib.LCB_PREC_MIXED, 3e-5)])
+@pytest.mark.parametrize("N", [33, 129, 257, 513])
+def test_compute_fields_sizes_vs_oracle(N, precision, rel):
+    """Random currents at several grid sizes, up to the production grid 513
+    (every tiling of the tensor-core waves: 32- and 64-wide tiles, eight and
+    four slices, the stage counts of each grid)."""
     L = _lib.load()
     h, dxi = 0.05, 0.05
     rng = np.random.default_rng(N)
@@ -248,15 +252,16 @@ def test_compute_fields_sizes_vs_oracle(N):
         d["cp_" + k], d["cf_" + k] = getattr(cp, k), getattr(cf, k)
     for k in ("Ex", "Ey", "Ez", "Bx", "By", "Bz", "Phi"):
         d["in_" + k], d["prev_" + k] = getattr(F, k), getattr(Fp, k)
-    ops = FieldOperators(N, h, 1 + dxi, DEV, False)
+    ops = FieldOperators(N, h, 1 + dxi, DEV, precision == _lib.LCB_PREC_MIXED)
     outs = [torch.zeros((7, N, N), dtype=torch.float64, device=DEV) for _ in range(2)]
-    ws = torch.empty(L.lcb_compute_fields_workspace_bytes(N, 0), dtype=torch.uint8, device=DEV)
-    a, keep = _fields_args(d, 0, ops, outs, ws)
+    ws = torch.empty(L.lcb_compute_fields_workspace_bytes(N, precision), dtype=torch.uint8,
+                     device=DEV)
+    a, keep = _fields_args(d, precision, ops, outs, ws)
     _lib.check(L.lcb_compute_fields(C.byref(a), _lib.stream_handle()), "compute_fields")
     torch.cuda.synchronize()
     for i, k in enumerate(("Ex", "Ey", "Ez", "Bx", "By", "Bz", "Phi")):
-        close(N_(outs[0][i]), getattr(full, k), 1e-11, f"N={N} full {k}")
-        close(N_(outs[1][i]), getattr(half, k), 1e-11, f"N={N} half {k}")
+        close(N_(outs[0][i]), getattr(full, k), rel, f"N={N} full {k}")
+        close(N_(outs[1][i]), getattr(half, k), rel, f"N={N} half {k}")
 
 
 def test_beam_deposit_and_substepping(kat):
@@ -421,3 +426,68 @@ def test_field_operators_build(N, mixed):
             got = buf[off:off + shp[0] * ld].reshape(shp[0], ld)[:, :shp[1]]
             rel_b = rel
         close(got.astype(np.float64), ref, rel_b, f"operator block {i}")
+
+
+@pytest.mark.parametrize("tag", ["t1", "t5"])
+def test_beam_move_vs_reference_kernel(golden, tag):
+    """lcb_beam_substepping + lcb_beam_move against the reference's own GPU
+    kernels (calculate_substepping_step and move_beam_cupy, compiled for the
+    host from the reference's sources: tests/golden/make_ref_kernel_golden.py)
+    on a layer with particles that stay, fall to the next layer and are lost."""
+    d = golden("kat_ref_beam.npz")
+    L = _lib.load()
+    N, h, dxi, layer, fell_size, time_step, sub_e = d[f"{tag}_params"]
+    N, layer, fell_size = int(N), int(layer), int(fell_size)
+    g = {k: T(d[f"{tag}_in_{k}"]) for k in ("xi", "x", "y", "px", "py", "pz", "q_m", "dt")}
+    g["id"] = T(d[f"{tag}_in_id"], torch.int64)
+    g["rs"] = T(d[f"{tag}_in_remaining_steps"], torch.int64)
+    n = g["x"].numel()
+    _lib.check(L.lcb_beam_substepping(n - fell_size, g["q_m"].data_ptr(), g["pz"].data_ptr(),
+                                      float(sub_e), float(time_step), g["dt"].data_ptr(),
+                                      g["rs"].data_ptr(), _lib.stream_handle()), "k6")
+    keys = ("Ex", "Ey", "Ez", "Bx", "By", "Bz")
+    fk = [T(d[f"{tag}_fk_{k}"]) for k in keys] + [torch.zeros(N, N, dtype=torch.float64, device=DEV)]
+    fk1 = [T(d[f"{tag}_fk1_{k}"]) for k in keys] + [torch.zeros(N, N, dtype=torch.float64, device=DEV)]
+    s0, s1 = _lib.Fields7(), _lib.Fields7()
+    for i in range(7):
+        s0.f[i], s1.f[i] = fk[i].data_ptr(), fk1[i].data_ptr()
+    flags = torch.zeros(n, dtype=torch.uint8, device=DEV)
+    err = torch.zeros(1, dtype=torch.int32, device=DEV)
+    R = h * N / 2
+    _lib.check(L.lcb_beam_move(n, float(dxi), max(0.9 * R, R - 1), layer - 1, float(h), N,
+                               g["q_m"].data_ptr(), g["dt"].data_ptr(), s0, s1,
+                               g["rs"].data_ptr(), g["id"].data_ptr(), g["x"].data_ptr(),
+                               g["y"].data_ptr(), g["xi"].data_ptr(), g["px"].data_ptr(),
+                               g["py"].data_ptr(), g["pz"].data_ptr(), flags.data_ptr(),
+                               err.data_ptr(), _lib.stream_handle()), "k5")
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    fl = N_(flags)
+    np.testing.assert_array_equal((fl & 1) != 0, d[f"{tag}_lost"])
+    np.testing.assert_array_equal((fl & 2) != 0, d[f"{tag}_moved"])
+    np.testing.assert_array_equal((fl & 4) != 0, d[f"{tag}_fell"])
+    np.testing.assert_array_equal(N_(g["id"]), d[f"{tag}_out_id"])
+    np.testing.assert_array_equal(N_(g["rs"]), d[f"{tag}_out_remaining_steps"])
+    np.testing.assert_array_equal(N_(g["dt"]), d[f"{tag}_out_dt"])
+    for k in ("x", "y", "xi", "px", "py", "pz"):
+        close(N_(g[k]), d[f"{tag}_out_{k}"], 1e-11, k)
+
+
+def test_beam_deposit_vs_reference_kernel(golden):
+    """lcb_beam_deposit against the reference's deposit_beam_cupy (compiled
+    for the host from the reference's sources)."""
+    d = golden("kat_ref_beam.npz")
+    L = _lib.load()
+    N, h, dxi, layer = d["dep_params"]
+    N, layer = int(N), int(layer)
+    x, y, xi, q = (T(d[k]) for k in ("dep_x", "dep_y", "dep_xi", "dep_q"))
+    r0 = T(d["dep_ro0_in"])
+    r1 = torch.zeros(N, N, dtype=torch.float64, device=DEV)
+    err = torch.zeros(1, dtype=torch.int32, device=DEV)
+    _lib.check(L.lcb_beam_deposit(x.numel(), N, float(h), float(dxi), layer, x.data_ptr(),
+                                  y.data_ptr(), xi.data_ptr(), q.data_ptr(), r0.data_ptr(),
+                                  r1.data_ptr(), err.data_ptr(), _lib.stream_handle()), "k4")
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    close(N_(r0), d["dep_ro0"], 1e-12, "ro0")
+    close(N_(r1), d["dep_ro1"], 1e-12, "ro1")

@@ -256,3 +256,162 @@ def test_resume_from_a_stored_plasma_state(tmp_path):
     ez_resumed = sim2.push_solver.ez_axis.cpu().numpy()
     assert ez_resumed.shape == ez_all[k_store + 1:].shape
     assert rel_err(ez_resumed, ez_all[k_store + 1:]) < 1e-10
+
+
+def _production_beam(shift=2.9):
+    """The production workload's seeded 1M-particle bi-Gaussian driver
+    (sigma_r 0.5, sigma_z 1, peak n_b/n0 0.5, gamma 1000 +- 1 %, emittance
+    1e-2), moved forward by `shift` in xi so that a short window starts inside
+    the beam; particles that end up ahead of xi = 0 are dropped."""
+    from lcodepy_b200.batch import bigaussian_beam
+    b = bigaussian_beam(1_000_000, 2024, 0.5, 1.0, -3.0, 1000.0, 0.01, 1e-2, -0.5, 0.02, 4.0)
+    b['xi'] += shift
+    return b[b['xi'] < 0]
+
+
+@pytest.mark.parametrize("precision,rel", [("fp64", 1e-8), ("mixed", 1e-5)])
+def test_production_configuration_vs_oracle(tmp_path, precision, rel):
+    """The benchmarked production grid (N=513, h 0.02, dxi 0.02, 929,296
+    electrons, background ions) with the production beam, pushed every
+    layer: 16 xi steps inside the beam, every layer with beam particles.
+    FP64: on-axis Ez, the final fields and the drained beam against the
+    oracle within 1e-8 relative.  Mixed precision: on-axis Ez relative L2 and
+    the final Ez within 1e-5 of the FP64 oracle."""
+    beam = _production_beam()
+    path = tmp_path / "beam.npz"
+    np.savez(path, **{k: beam[k] for k in beam.dtype.names})
+    config = {'geometry': '3d', 'processing-unit-type': 'gpu', 'window-width': 5.13,
+              'transverse-step': 0.02, 'window-length': 0.3, 'xi-step': 0.02,
+              'time-limit': 1.0, 'time-step': 1.0, 'ion-model': 'background',
+              'plasma-particles-per-cell': 4, 'print-every': 0, 'precision': precision}
+    sim = Simulation(config=config, beam_parameters={}, diagnostics=[], runas_filename='')
+    sim.load_beamfile(str(path))
+    sim.step(1)
+    ps = sim.push_solver
+    particles, fields, currents = ps._plasmastate
+    ez = ps.ez_axis.cpu().numpy()
+    N = fields.Ez.shape[0]
+    assert N == 513 and ez.size == 16
+
+    p = O.make_params(5.13, 0.02, 0.02)
+    sorts, consts = O.init_plasma(p)
+    F, cur = O.Fields.zeros(p.N), O.Currents.zeros(p.N)
+    ez_o, layers = [], []
+    ob = O.Beam.from_array(beam).sorted()
+    sorts, F, cur, drain = O.step_dt(
+        p, sorts, F, cur, consts, 15, beam=ob, time_step=1.0,
+        record=lambda i, s, f, c, rb: (ez_o.append(f.Ez[p.N // 2, p.N // 2]),
+                                       layers.append(np.abs(rb).max())))
+    ez_o = np.array(ez_o)
+    assert min(layers[1:]) > 0   # the beam is present in every layer
+    if precision == "fp64":
+        assert rel_err(ez, ez_o) < rel
+        for k in ("Ex", "Ey", "Ez", "Bx", "By", "Bz", "Phi"):
+            assert rel_err(getattr(fields, k).cpu().numpy(), getattr(F, k)) < rel, k
+        e = particles["electrons"]
+        for k in ("x_offt", "y_offt", "px", "py", "pz"):
+            assert rel_err(getattr(e, k).cpu().numpy(), getattr(sorts[0], k)) < rel, k
+        got = sim.beam_drain.beam_slice()
+        gid = got.id.cpu().numpy()
+        assert gid.size == drain.id.size and gid.size > 0
+        order, ref_order = np.argsort(gid), np.argsort(drain.id)
+        np.testing.assert_array_equal(gid[order], drain.id[ref_order])
+        for k in ("x", "y", "xi", "px", "py", "pz"):
+            assert rel_err(getattr(got, k).cpu().numpy()[order],
+                           getattr(drain, k)[ref_order]) < rel, k
+    else:
+        l2 = np.linalg.norm(ez - ez_o) / np.linalg.norm(ez_o)
+        print(f"N=513 production beam, mixed vs FP64 oracle: on-axis Ez rel L2 {l2:.2e}")
+        assert l2 < rel
+        assert np.linalg.norm(fields.Ez.cpu().numpy() - F.Ez) / np.linalg.norm(F.Ez) < rel
+
+
+class _SliceRecorder:
+    """A diagnostic with the reference's after_step_dxi signature that keeps
+    on-axis Ez every xi step and the rho (sorts summed) and Ez slices every
+    `every` xi steps."""
+
+    def __init__(self, every=20):
+        self.every = every
+
+    def pull_config(self, config):
+        self.k, self.rho, self.ez = 0, [], []
+
+    def after_step_dxi(self, t, xi, particles, fields, currents, rho_beam):
+        if self.k % self.every == 0:
+            self.rho.append(currents.ro.get().sum(axis=0))
+            self.ez.append(fields.Ez.get())
+        self.k += 1
+
+    def dump(self, *a, **k):
+        pass
+
+
+def _rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def test_mixed_precision_slices_and_axis():
+    """The precision form of the 129 x 129 rigid configuration (201 xi steps):
+    on-axis Ez over the run, and the rho (sorts summed) and Ez slices taken
+    every 20 xi steps, over the run, within relative L2 1e-5 of the FP64 run.
+    The per-slice errors are printed too; the first rho slice, at xi = 0, is
+    the small first response of a neutral plasma (electrons and ions cancel),
+    so its own relative error is larger than the run's."""
+    base = cfg(**{'rigid-beam': True, 'window-width': 6.5, 'transverse-step': 0.1,
+                  'xi-step': 0.1, 'window-length': 20})
+    out = {}
+    for prec in ("fp64", "mixed"):
+        rec = _SliceRecorder(20)
+        sim = Simulation(config={**base, 'precision': prec}, beam_parameters=rigid_driver,
+                         diagnostics=[rec], runas_filename='')
+        sim.step()
+        out[prec] = (sim.push_solver.ez_axis.cpu().numpy(), rec)
+    ez64, r64 = out["fp64"]
+    ezmx, rmx = out["mixed"]
+    assert len(r64.rho) == 11
+    e_axis = _rel_l2(ezmx, ez64)
+    e_rho = _rel_l2(np.stack(rmx.rho), np.stack(r64.rho))
+    e_ez = _rel_l2(np.stack(rmx.ez), np.stack(r64.ez))
+    per_rho = [_rel_l2(a, b) for a, b in zip(rmx.rho, r64.rho)]
+    per_ez = [_rel_l2(a, b) for a, b in zip(rmx.ez[1:], r64.ez[1:])]
+    print(f"mixed vs FP64, 129^2 201 steps: on-axis Ez {e_axis:.2e}; rho slices {e_rho:.2e} "
+          f"(per slice {' '.join(f'{e:.1e}' for e in per_rho)}); Ez slices {e_ez:.2e} "
+          f"(per slice max {max(per_ez):.1e})")
+    assert e_axis < 1e-5
+    assert e_rho < 1e-5
+    assert e_ez < 1e-5
+
+
+def test_mixed_precision_beam_energy():
+    """The precision form with a non-rigid beam (129 x 129, two time steps of
+    5, a generated gamma ~ 10 beam): the drained beam's mean energy, and its
+    change over the run, within 1e-5 relative of the FP64 run; on-axis Ez of
+    the second time step within relative L2 1e-5."""
+    base = cfg(**{'window-width': 6.5, 'transverse-step': 0.1, 'xi-step': 0.1,
+                  'window-length': 8, 'time-limit': 2, 'time-step': 5.0})
+    beam = {'current': -0.5, 'particles_in_layer': 500,
+            'default': {'length': 4.0, 'energy': 10.0, 'angspread': 1e-2}}
+    res = {}
+    for prec in ("fp64", "mixed"):
+        sim, _, _, _, ez = run({**base, 'precision': prec}, beam, n_steps=2)
+        b = sim.beam_drain.beam_slice()
+        p2 = b.px.cpu().numpy() ** 2 + b.py.cpu().numpy() ** 2 + b.pz.cpu().numpy() ** 2
+        energy = np.sqrt(1 / b.q_m.cpu().numpy() ** 2 + p2)
+        res[prec] = (ez, energy, b.id.cpu().numpy())
+    ez64, en64, id64 = res["fp64"]
+    ezmx, enmx, idmx = res["mixed"]
+    np.testing.assert_array_equal(np.sort(id64), np.sort(idmx))
+    from lcodepy_b200.beam_generator import generate_beam
+    from lcodepy_b200.config import Config
+    c = Config(base)
+    c._adjust_config_values_3d()
+    g = generate_beam(c, beam)
+    e0 = np.sqrt(1 / g['q_m'] ** 2 + g['px'] ** 2 + g['py'] ** 2 + g['pz'] ** 2).mean()
+    m64, mmx = en64.mean(), enmx.mean()
+    e_mean = abs(mmx - m64) / m64
+    e_change = abs(mmx - m64) / abs(m64 - e0)
+    e_axis = _rel_l2(ezmx, ez64)
+    print(f"mixed vs FP64 beam: mean energy {e_mean:.2e}, energy change {e_change:.2e} "
+          f"(FP64 change {m64 - e0:.3e} of {e0:.3f}), on-axis Ez {e_axis:.2e}")
+    assert e_mean < 1e-5 and e_change < 1e-5 and e_axis < 1e-5

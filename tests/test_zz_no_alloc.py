@@ -23,7 +23,10 @@ from lcodepy_b200 import _lib  # noqa: E402
 from lcodepy_b200.plasma3d import FieldOperators  # noqa: E402
 
 DEV = torch.device("cuda")
-REL = 1e-11  # compute_fields FP64 tolerance used in tests/test_gpu_kernels.py
+# the compute_fields tolerances of tests/test_gpu_kernels.py, per precision
+REL = {_lib.LCB_PREC_FP64: 1e-11, _lib.LCB_PREC_MIXED: 3e-5}
+# the largest grid whose scratch fits the fixed array, per precision
+LIMIT = {_lib.LCB_PREC_FP64: 283, _lib.LCB_PREC_MIXED: 427}
 
 
 def _inputs(N, seed):
@@ -44,9 +47,10 @@ def _inputs(N, seed):
                 rbp=torch.tensor(rng.normal(0, 1, (N, N)), device=DEV))
 
 
-def _args(N, h, dxi, ops, inp, out_full, out_half, ws=None):
+def _args(N, h, dxi, ops, inp, out_full, out_half, ws=None, precision=0):
     a = _lib.ComputeFieldsArgs()
-    a.grid_steps, a.h, a.xi_step, a.subtraction_coeff, a.precision = N, h, dxi, 1 + dxi, 0
+    a.grid_steps, a.h, a.xi_step, a.subtraction_coeff = N, h, dxi, 1 + dxi
+    a.precision = precision
     a.operators = ops.ptr
     for i in range(7):
         a.fields.f[i] = inp["F"][i].data_ptr()
@@ -67,35 +71,42 @@ def _rel(a, b):
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
 
 
-@pytest.mark.parametrize("N", [129, 257])
-def test_noalloc_matches_workspace_entry_point_twice(N):
+@pytest.mark.parametrize("precision,N", [(_lib.LCB_PREC_FP64, 129), (_lib.LCB_PREC_FP64, 257),
+                                         (_lib.LCB_PREC_FP64, 283), (_lib.LCB_PREC_MIXED, 129),
+                                         (_lib.LCB_PREC_MIXED, 427)])
+def test_noalloc_matches_workspace_entry_point_twice(precision, N):
     L = _lib.load()
     h, dxi = 0.05, 0.05
-    ops = FieldOperators(N, h, 1 + dxi, DEV, False)
+    assert L.lcb_compute_fields_workspace_bytes(LIMIT[precision], precision) <= \
+        _lib.LCB_NOALLOC_FIELDS_SCRATCH_BYTES < \
+        L.lcb_compute_fields_workspace_bytes(LIMIT[precision] + 2, precision)
+    ops = FieldOperators(N, h, 1 + dxi, DEV, precision == _lib.LCB_PREC_MIXED)
     for call, seed in enumerate((N, N + 1)):  # two calls in a row, different inputs
         inp = _inputs(N, seed)
         ref_full = torch.zeros(7, N, N, dtype=torch.float64, device=DEV)
         ref_half = torch.zeros_like(ref_full)
-        ws = torch.empty(L.lcb_compute_fields_workspace_bytes(N, 0), dtype=torch.uint8,
+        ws = torch.empty(L.lcb_compute_fields_workspace_bytes(N, precision), dtype=torch.uint8,
                          device=DEV)
-        a = _args(N, h, dxi, ops, inp, ref_full, ref_half, ws)
+        a = _args(N, h, dxi, ops, inp, ref_full, ref_half, ws, precision)
         _lib.check(L.lcb_compute_fields(C.byref(a), _lib.stream_handle()), "compute_fields")
         got_full = torch.full((7, N, N), 5.0, dtype=torch.float64, device=DEV)
         got_half = torch.full((7, N, N), 5.0, dtype=torch.float64, device=DEV)
-        b = _args(N, h, dxi, ops, inp, got_full, got_half)  # no workspace given
+        b = _args(N, h, dxi, ops, inp, got_full, got_half, None, precision)  # no workspace
         _lib.check(L.lcb_compute_fields_noalloc(C.byref(b), _lib.stream_handle()),
                    "compute_fields_noalloc")
         torch.cuda.synchronize()
         for i in range(7):
-            assert _rel(got_full[i], ref_full[i]) <= REL, (call, i, "full")
-            assert _rel(got_half[i], ref_half[i]) <= REL, (call, i, "half")
+            assert _rel(got_full[i], ref_full[i]) <= REL[precision], (call, i, "full")
+            assert _rel(got_half[i], ref_half[i]) <= REL[precision], (call, i, "half")
 
 
-def test_noalloc_rejects_grids_beyond_its_scratch():
+@pytest.mark.parametrize("precision", [_lib.LCB_PREC_FP64, _lib.LCB_PREC_MIXED])
+def test_noalloc_rejects_grids_beyond_its_scratch(precision):
     L = _lib.load()
-    a = _lib.ComputeFieldsArgs()
-    a.grid_steps, a.precision = 513, 0
-    rc = L.lcb_compute_fields_noalloc(C.byref(a), _lib.stream_handle())
-    assert rc == 1
-    msg = L.lcb_last_error().decode()
-    assert "513" in msg and "scratch" in msg
+    for N in (LIMIT[precision] + 2, 513):
+        a = _lib.ComputeFieldsArgs()
+        a.grid_steps, a.precision = N, precision
+        rc = L.lcb_compute_fields_noalloc(C.byref(a), _lib.stream_handle())
+        assert rc == 1
+        msg = L.lcb_last_error().decode()
+        assert str(N) in msg and "scratch" in msg
