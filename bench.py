@@ -395,7 +395,7 @@ def run_serve(args, ws, rank, local):
     arrivals and the measured durations."""
     import torch
     from lcodepy_b200 import _lib
-    from lcodepy_b200.batch import Server, request_stream
+    from lcodepy_b200.batch import BeamDriver, Server, request_stream
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     reqs = request_stream(n=args.requests, precision=args.precision)

@@ -28,6 +28,7 @@
 // All products run on the int8 tensor cores (tcgen05) on sliced operands,
 // exactly: eight slices reproduce FP64 accuracy, four FP32 accuracy (mixed
 // precision).
+#include <cstdlib>
 #include <cstring>
 
 #include "common.cuh"
@@ -110,14 +111,17 @@ struct OpLayout {
 
 
 // ---------------------------------------------------------------------------
-// Mixed precision operand storage: four int8 slice planes per matrix, each
-// plane cut into the tiles the tensor-core GEMM streams (zero padded), each
-// tile stored in the tensor cores' no-swizzle core-matrix order so that one
-// contiguous bulk copy fills a shared-memory stage.
-//   A role (M x K, K-major): 128 x 32 tiles of 4096 bytes, tile (mt, kt) at
-//     (mt KT + kt) 4096, element (r, k) at (r/8) 256 + (k/16) 128 + (r%8) 16 + k%16;
-//   B role (K x N, N-major): 32 x 64 tiles of 2048 bytes, tile (kt, nt) at
-//     (nt KT + kt) 2048, element (k, n) at (n/16) 512 + (k/8) 128 + (k%8) 16 + n%16.
+// Operand storage: NS int8 slices per element (four for mixed precision,
+// eight for FP64), cut into the tiles the tensor-core GEMM streams (zero
+// padded), each tile stored in the tensor cores' no-swizzle core-matrix
+// order, and the NS slices of a tile back to back, so that one contiguous
+// bulk copy fills a shared-memory stage.
+//   A role (M x K, K-major): 128 x 32 tiles of 4096 bytes per slice, slice i
+//     of tile (mt, kt) at ((mt KT + kt) NS + i) 4096, element (r, k) at
+//     (r/8) 256 + (k/16) 128 + (r%8) 16 + k%16;
+//   B role (K x N, N-major): 32 x 64 tiles of 2048 bytes per slice, slice i
+//     of tile (kt, nt) at ((nt KT + kt) NS + i) 2048, element (k, n) at
+//     (n/16) 512 + (k/8) 128 + (k%8) 16 + n%16.
 // ---------------------------------------------------------------------------
 constexpr int TL_M = 128, TL_K = 32, TL_N = 64;
 __host__ __device__ constexpr int ntiles(int x, int t) { return (x + t - 1) / t; }
@@ -129,14 +133,17 @@ __host__ __device__ constexpr int64_t b_plane_bytes(int K, int N)
 {
     return (int64_t)ntiles(K, TL_K) * ntiles(N, TL_N) * (TL_K * TL_N);
 }
-__host__ __device__ inline int64_t a_tile_off(int r, int k, int KT)
+// Offset of slice i of element (r, k) (A role) or (k, n) (B role): the NS
+// slices of one tile are stored back to back, so that a stage of the
+// tensor-core pipeline is one contiguous copy per operand.
+__host__ __device__ inline int64_t a_tile_off(int r, int k, int KT, int NS, int i)
 {
-    return ((int64_t)((r >> 7) * KT + (k >> 5)) << 12) + ((r & 127) >> 3) * 256 +
+    return ((((int64_t)(r >> 7) * KT + (k >> 5)) * NS + i) << 12) + ((r & 127) >> 3) * 256 +
            ((k & 31) >> 4) * 128 + (r & 7) * 16 + (k & 15);
 }
-__host__ __device__ inline int64_t b_tile_off(int k, int n, int KT)
+__host__ __device__ inline int64_t b_tile_off(int k, int n, int KT, int NS, int i)
 {
-    return ((int64_t)((n >> 6) * KT + (k >> 5)) << 11) + ((n & 63) >> 4) * 512 +
+    return ((((int64_t)(n >> 6) * KT + (k >> 5)) * NS + i) << 11) + ((n & 63) >> 4) * 512 +
            ((k & 31) >> 3) * 128 + (k & 7) * 16 + (n & 15);
 }
 
@@ -230,7 +237,6 @@ __global__ void k_build_slices(int N, OpLayout L, uint8_t *bytes)
     for (int b = 0; b < OP_D; b++) {
         const bool a_role = b == OP_SE || b == OP_SO || b == OP_CE || b == OP_CO;
         const int R = (int)L.rows[b], C = (int)L.cols[b];
-        const int64_t plane = a_role ? a_plane_bytes(R, C) : b_plane_bytes(R, C);
         // padded extents: A role 128-row x 32-col tiles, B role 32 x 64
         const int Rp = a_role ? ntiles(R, TL_M) * TL_M : ntiles(R, TL_K) * TL_K;
         const int Cp = a_role ? ntiles(C, TL_K) * TL_K : ntiles(C, TL_N) * TL_N;
@@ -254,9 +260,9 @@ __global__ void k_build_slices(int N, OpLayout L, uint8_t *bytes)
             }
             unsigned sl[NS];
             slices_of<NS>(v, 0.5, sl);
-            const int64_t at = a_role ? a_tile_off(r, q, KT) : b_tile_off(r, q, KT);
 #pragma unroll
-            for (int i = 0; i < NS; i++) base[i * plane + at] = (uint8_t)sl[i];
+            for (int i = 0; i < NS; i++)
+                base[a_role ? a_tile_off(r, q, KT, NS, i) : b_tile_off(r, q, KT, NS, i)] = (uint8_t)sl[i];
         }
     }
 }
@@ -278,15 +284,19 @@ struct GemmDesc {
     // by the fold pass that produced it); NULL for a transform block, whose
     // elements are bounded by 2
     const unsigned *amax_a, *amax_b;
-    // mixed precision: A and B are four tiled int8 slice planes (A role and
-    // B role); a_plane / b_plane are the plane strides in bytes
-    int a_plane, b_plane;
     // which operand is a transform block (1: A, 2: B), whose copies may be
     // issued before the predecessor kernel has finished
     int const_op;
 };
 
 enum Epi { EPI_STORE = 0, EPI_SCALE = 1, EPI_FIELD = 2 };
+
+// The fields of a product that its epilogue reads, held in registers.
+template <typename T>
+struct EpiDesc {
+    T *C; const T *E;
+    int ldc, lde, rmul, radd, cmul, cadd, M, N;
+};
 
 struct FieldOut {
     double *half, *full;      // may be NULL
@@ -303,6 +313,7 @@ struct GemmBatch {
     GemmDesc<T> d[MAXSUB];
     FieldOut out[NPROB];
     int grid_n;
+    int nsub;             // products in d (the persistent wave walks their tiles)
     unsigned *amax_out;   // mixed: per-problem max |stored value| (zeroed), or NULL
 };
 
@@ -397,23 +408,21 @@ __device__ __forceinline__ bool mbar_wait(unsigned mbar, unsigned parity)
 
 // Epilogue of the integer products, split so that a group of outputs can
 // load what it needs (scale factor, previous field) before storing.
-template <int EPI, typename T>
-__device__ __forceinline__ double epi_pre(const GemmBatch<T> &b, const GemmDesc<T> &g,
-                                          int m, int n)
+template <int EPI, typename T, typename G>
+__device__ __forceinline__ double epi_pre(const FieldOut &o, int grid_n, const G &g, int m, int n)
 {
     const int om = g.rmul * m + g.radd, on = g.cmul * n + g.cadd;
     if (EPI == EPI_SCALE) return (double)g.E[(int64_t)om * g.lde + on];
     if (EPI == EPI_FIELD) {
-        const FieldOut &o = b.out[g.prob];
         if ((o.kind == 0 && o.full) || (o.kind == 1 && o.half))
-            return o.prev[(int64_t)(om + o.row_off) * b.grid_n + on + o.col_off];
+            return o.prev[(int64_t)(om + o.row_off) * grid_n + on + o.col_off];
     }
     return 0.0;
 }
 
-template <int EPI, typename T>
-__device__ __forceinline__ double epi_apply(const GemmBatch<T> &b, const GemmDesc<T> &g,
-                                            int m, int n, T v, double pre, float &vmax)
+template <int EPI, typename T, typename G>
+__device__ __forceinline__ double epi_apply(const FieldOut &o, int grid_n, const G &g, int m, int n,
+                                            T v, double pre, float &vmax)
 {
     const int om = g.rmul * m + g.radd, on = g.cmul * n + g.cadd;
     if (EPI == EPI_STORE) {
@@ -424,8 +433,7 @@ __device__ __forceinline__ double epi_apply(const GemmBatch<T> &b, const GemmDes
         g.C[(int64_t)om * g.ldc + on] = st;
         vmax = fmaxf(vmax, abs_bound(st));
     } else {
-        const FieldOut &o = b.out[g.prob];
-        const int64_t off = (int64_t)(om + o.row_off) * b.grid_n + on + o.col_off;
+        const int64_t off = (int64_t)(om + o.row_off) * grid_n + on + o.col_off;
         const double dv = (double)v;
         if (o.kind == 0) {
             if (o.half) o.half[off] = dv;
@@ -489,13 +497,13 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
     if (m0 >= M || n0 >= N) return;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int KT = ntiles(K, TL_K);
-    // this CTA's tile rows of A and tile column of B
-    const uint8_t *At = reinterpret_cast<const uint8_t *>(g.A) + (int64_t)blockIdx.y * KT * I8_A_SLICE;
-    const uint8_t *Bt = reinterpret_cast<const uint8_t *>(g.B) + (int64_t)(n0 / TL_N) * KT * (TL_K * TL_N) +
+    // this CTA's tile rows of A and tile column of B (NS slices per tile)
+    const uint8_t *At = reinterpret_cast<const uint8_t *>(g.A) + (int64_t)blockIdx.y * KT * NS * I8_A_SLICE;
+    const uint8_t *Bt = reinterpret_cast<const uint8_t *>(g.B) + (int64_t)(n0 / TL_N) * KT * NS * (TL_K * TL_N) +
                         ((n0 % TL_N) >> 4) * 512;
     // BN = 128: the second B tile column (or the first again past the last
     // one; its products land in columns that are never stored)
-    const uint8_t *Bt2 = (n0 / TL_N + 1) < ntiles(N, TL_N) ? Bt + (int64_t)KT * (TL_K * TL_N) : Bt;
+    const uint8_t *Bt2 = (n0 / TL_N + 1) < ntiles(N, TL_N) ? Bt + (int64_t)KT * NS * (TL_K * TL_N) : Bt;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -526,16 +534,14 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
 #pragma unroll
         for (int i = 0; i < NS; i++) {
             if (part & 1)
-                bulk_g2s(sA + i * I8_A_SLICE, At + (int64_t)i * g.a_plane + (int64_t)kt * I8_A_SLICE,
-                         I8_A_SLICE, mb);
+                bulk_g2s(sA + i * I8_A_SLICE, At + ((int64_t)kt * NS + i) * I8_A_SLICE, I8_A_SLICE, mb);
             if (part & 2) {
                 if constexpr (BN > TL_N) {
                     constexpr int HB = TL_K * TL_N;   // one 64-wide tile slice
-                    bulk_g2s(sB + i * Cfg::B_SLICE, Bt + (int64_t)i * g.b_plane + (int64_t)kt * HB, HB, mb);
-                    bulk_g2s(sB + i * Cfg::B_SLICE + HB, Bt2 + (int64_t)i * g.b_plane + (int64_t)kt * HB, HB,
-                             mb);
+                    bulk_g2s(sB + i * Cfg::B_SLICE, Bt + ((int64_t)kt * NS + i) * HB, HB, mb);
+                    bulk_g2s(sB + i * Cfg::B_SLICE + HB, Bt2 + ((int64_t)kt * NS + i) * HB, HB, mb);
                 } else {
-                    bulk_g2s(sB + i * Cfg::B_SLICE, Bt + (int64_t)i * g.b_plane + (int64_t)kt * (TL_K * TL_N),
+                    bulk_g2s(sB + i * Cfg::B_SLICE, Bt + ((int64_t)kt * NS + i) * (TL_K * TL_N),
                              Cfg::B_SLICE, mb);
                 }
             }
@@ -564,7 +570,8 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
     for (int it = 0; it < CW; it++) {
         const int e = it * 32 + lane, row = e / CW, col = e % CW;
         const int gm = m0 + 32 * rq + row, gn = n0 + CW * ch + col;
-        pre[it] = (EPI != EPI_STORE && gm < M && gn < N) ? epi_pre<EPI, T>(batch, g, gm, gn) : 0.0;
+        pre[it] = (EPI != EPI_STORE && gm < M && gn < N)
+                      ? epi_pre<EPI, T>(batch.out[g.prob], batch.grid_n, g, gm, gn) : 0.0;
     }
 
     bool ok = true;
@@ -656,7 +663,8 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
         const int e = it * 32 + lane, row = e / CW, col = e % CW;
         const int gm = m0 + 32 * rq + row, gn = n0 + CW * ch + col;
         if (gm >= M || gn >= N) continue;
-        part += epi_apply<EPI, T>(batch, g, gm, gn, stage[row * (CW + 1) + col], pre[it], vmax);
+        part += epi_apply<EPI, T>(batch.out[g.prob], batch.grid_n, g, gm, gn, stage[row * (CW + 1) + col],
+                                  pre[it], vmax);
     }
     if (EPI != EPI_FIELD && batch.amax_out) {
 #pragma unroll
@@ -669,6 +677,365 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
                      :: "r"(tmem), "r"(Cfg::TMEM_COLS) : "memory");
     if (EPI == EPI_FIELD && batch.out[g.prob].kind == 3) bz_reduce<Cfg::THREADS>(part, batch.out[g.prob].bz_sum);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent, warp-specialised form of the transform waves.  One CTA per SM
+// walks a static share of the wave's output tiles (every product of the wave
+// in one list, tile t on CTA t mod grid).  Warp 0 streams the operand stages
+// (one lane issues the bulk copies), warp 1 issues the MMAs, warps 4-11 read
+// tensor memory, combine and store.
+//
+// Wide slice products: the B slices of a stage lie side by side in shared
+// memory (slice j at columns j bn .. j bn + bn - 1 of one N-major operand), so
+// the products of A slice i with B slices 0 .. NS-1-i are one MMA of
+// N = (NS - i) bn columns whose accumulator starts at column block i: the
+// product A_i B_j lands in block i + j, the accumulator of its weight.  NS
+// MMAs of up to 256 columns (split where wider) replace NS (NS + 1) / 2
+// narrow ones, and every A slice is read from shared memory once per MMA
+// instead of once per B slice.
+//
+// Tensor memory holds 512 / (NS bn) accumulator sets: with four slices two
+// sets alternate, so a tile's epilogue overlaps the next tile's main loop;
+// with eight slices the one set is released as soon as the epilogue warps
+// hold the combined values in registers, before they store them.
+//
+// The last tile column of a product narrower than a multiple of 64 uses a
+// narrower tile (16, 32 or 48 columns): less operand traffic and fewer MMA
+// columns for the padding.
+// ---------------------------------------------------------------------------
+constexpr int WP_BN = 64;                 // widest tile (columns)
+constexpr int WP_EPI_WARP0 = 4;           // warps 4 .. 11 run the epilogue
+constexpr int WP_EPI_WARPS = 8;
+constexpr int WP_THREADS = 32 * (WP_EPI_WARP0 + WP_EPI_WARPS);
+
+// KS k tiles (of 32) per pipeline stage: one barrier round trip and one
+// commit per KS x NS wide MMAs.
+template <int NS, int KS>
+struct WPCfg {
+    static constexpr int B_TILE = I8_BK * WP_BN;               // bytes per B slice (64 wide)
+    static constexpr int KSTAGE = NS * (I8_A_SLICE + B_TILE);  // one k tile: 24 KB (4 slices) / 48 KB (8)
+    static constexpr int STAGE = KS * KSTAGE;
+    static constexpr int ST = (144 * 1024) / STAGE;            // pipeline stages
+    static_assert(ST >= 2, "at least two pipeline stages");
+    static constexpr int SET_COLS = NS * WP_BN;                // 256 / 512 TMEM columns
+    static constexpr int NSETS = 512 / SET_COLS;               // 2 / 1 accumulator sets
+    static constexpr int CW = WP_BN / 2;                       // epilogue columns per warp (max)
+    // per epilogue warp a 32 x CW block of outputs (one padding column), so
+    // that the stores run along rows
+    static constexpr int EPI_BYTES = WP_EPI_WARPS * 32 * (CW + 1) * NS;
+    static constexpr size_t smem = (size_t)ST * STAGE + EPI_BYTES + 256;
+};
+
+// Instruction descriptor of kind::i8 (s32 accumulator, signed int8 A K-major,
+// B N-major), M = 128, N = n.
+__device__ __forceinline__ unsigned i8_idesc_n(int n)
+{
+    return (2u << 4) | (1u << 7) | (1u << 10) | (1u << 16) | ((unsigned)(n >> 3) << 17) |
+           ((unsigned)(I8_BM >> 4) << 24);
+}
+
+// Tile t of the batch: product s, tile row mt, tile column nt (nt fastest,
+// so that the tiles running together share their A row block in L2), from
+// the products' first tiles `tstart` (shared memory).
+template <typename T>
+__device__ __forceinline__ void wave_tile(const GemmDesc<T> *sd, const int *tstart, int nsub, int t,
+                                          int &s, int &mt, int &nt)
+{
+    s = 0;
+    while (s + 1 < nsub && t >= tstart[s + 1]) s++;
+    const int tn = ntiles(sd[s].N, WP_BN), r = t - tstart[s];
+    mt = r / tn;
+    nt = r - mt * tn;
+}
+
+// Width of tile column nt: 64, or the remaining columns rounded up to 16.
+__device__ __forceinline__ int wave_tile_bn(int N, int nt)
+{
+    const int rem = N - nt * WP_BN;
+    return rem >= WP_BN ? WP_BN : (rem + 15) & ~15;
+}
+
+// A bounded wait that also gives up as soon as another role of the CTA has
+// given up (`bad` set), so that a failed protocol ends the kernel quickly.
+__device__ __forceinline__ bool wp_wait(unsigned mbar, unsigned parity, volatile int *bad)
+{
+    for (int it = 0; it < (1 << 22); it++) {
+        unsigned done;
+        asm volatile("{\n.reg .pred P1;\nmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n"
+                     "selp.b32 %0, 1, 0, P1;\n}\n"
+                     : "=r"(done) : "r"(mbar), "r"(parity) : "memory");
+        if (done) return true;
+        if ((it & 255) == 255 && *bad) return false;
+    }
+    *bad = 1;
+    return false;
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned mbar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(mbar) : "memory");
+}
+
+template <typename T, int EPI, int KS>
+__global__ void __launch_bounds__(WP_THREADS, 1)
+k_wave_i8p(const __grid_constant__ GemmBatch<T> batch, int total)
+{
+    constexpr int NS = Slices<T>::n;
+    using Cfg = WPCfg<NS, KS>;
+    constexpr int ST = Cfg::ST, NSETS = Cfg::NSETS, CW = Cfg::CW;
+    extern __shared__ __align__(1024) uint8_t wpsm[];
+    T *epi_stage = reinterpret_cast<T *>(wpsm + ST * Cfg::STAGE);          // epilogue blocks
+    uint64_t *full = reinterpret_cast<uint64_t *>(wpsm + ST * Cfg::STAGE + Cfg::EPI_BYTES);  // [ST]
+    uint64_t *empty = full + ST;                                            // [ST] stage consumed
+    uint64_t *tfull = empty + ST;                                           // [NSETS] tile accumulated
+    uint64_t *tempty = tfull + NSETS;                                       // [NSETS] set drained
+    unsigned *tslot = reinterpret_cast<unsigned *>(tempty + NSETS);
+    int *bad = reinterpret_cast<int *>(tslot + 1);                          // a bounded wait gave up
+
+    // the products' descriptors and the field outputs, copied to shared
+    // memory once: every role reads them per tile, and dynamically indexed
+    // reads of the kernel parameters are slow and serialise
+    __shared__ GemmDesc<T> sd[MAXSUB];
+    __shared__ FieldOut so[NPROB];
+    __shared__ int tstart[MAXSUB + 1];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    {
+        const int *src = reinterpret_cast<const int *>(&batch.d[0]);
+        int *dst = reinterpret_cast<int *>(sd);
+        for (int i = tid; i < (int)(sizeof(sd) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+        const int *src2 = reinterpret_cast<const int *>(&batch.out[0]);
+        int *dst2 = reinterpret_cast<int *>(so);
+        for (int i = tid; i < (int)(sizeof(so) / sizeof(int)); i += blockDim.x) dst2[i] = src2[i];
+        if (tid == 0) {
+            int acc = 0;
+            for (int q = 0; q < batch.nsub; q++) {
+                tstart[q] = acc;
+                acc += ntiles(batch.d[q].M, I8_BM) * ntiles(batch.d[q].N, WP_BN);
+            }
+            tstart[batch.nsub] = acc;
+        }
+    }
+    const int nsub = batch.nsub, grid_n = batch.grid_n;
+    unsigned *const amax_out = batch.amax_out;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(tslot)), "r"(512) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int q = 0; q < 2 * ST + NSETS; q++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(full + q)), "r"(1)
+                         : "memory");
+        for (int q = 0; q < NSETS; q++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;"
+                         :: "r"(smem_u32(tempty + q)), "r"(WP_EPI_WARPS) : "memory");
+        *bad = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const unsigned tmem = *tslot;
+    volatile int *vbad = bad;
+    // every role reads or writes what the preceding kernels produce or read
+    pdl_wait();
+    pdl_trigger();
+
+    if (warp == 0) {
+        // ---- producer: two bulk copies per stage (A, B) ----
+        unsigned g = 0;
+        for (int t = blockIdx.x; t < total; t += gridDim.x) {
+            int s, mt, nt;
+            wave_tile(sd, tstart, nsub, t, s, mt, nt);
+            const GemmDesc<T> &d = sd[s];
+            const int KT = ntiles(d.K, TL_K), bn = wave_tile_bn(d.N, nt);
+            // the NS slices of a tile, and the tiles along k, are contiguous:
+            // one copy for A and one for B per stage (a narrow last tile
+            // column copies its columns of each slice)
+            const uint8_t *At = reinterpret_cast<const uint8_t *>(d.A) + (int64_t)mt * KT * NS * I8_A_SLICE;
+            const uint8_t *Bt = reinterpret_cast<const uint8_t *>(d.B) + (int64_t)nt * KT * NS * Cfg::B_TILE;
+            const unsigned bbytes = (unsigned)bn * I8_BK;
+            for (int k0 = 0; k0 < KT; k0 += KS, g++) {
+                const int ktn = KT - k0 < KS ? KT - k0 : KS;
+                const int buf = (int)(g % ST);
+                if (g >= (unsigned)ST) wp_wait(smem_u32(empty + buf), ((g / ST) - 1) & 1, vbad);
+                if (lane == 0) {
+                    const unsigned sA = smem_u32(wpsm + buf * Cfg::STAGE);
+                    const unsigned sB = sA + KS * NS * I8_A_SLICE;
+                    const unsigned mb = smem_u32(full + buf);
+                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;"
+                                 :: "r"((unsigned)(ktn * NS) * (I8_A_SLICE + bbytes)), "r"(mb) : "memory");
+                    bulk_g2s(sA, At + (int64_t)k0 * NS * I8_A_SLICE, ktn * NS * I8_A_SLICE, mb);
+                    const uint8_t *Bk = Bt + (int64_t)k0 * NS * Cfg::B_TILE;
+                    if (bn == WP_BN) {
+                        bulk_g2s(sB, Bk, ktn * NS * Cfg::B_TILE, mb);
+                    } else {
+                        for (int q = 0; q < ktn * NS; q++)
+                            bulk_g2s(sB + q * bbytes, Bk + q * Cfg::B_TILE, bbytes, mb);
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        // the last fill of every buffer has landed before the CTA may exit
+        for (int q = 0; q < ST && q < (int)g; q++) {
+            const unsigned last = g - 1 - (unsigned)q;
+            wp_wait(smem_u32(full + last % ST), (last / ST) & 1, vbad);
+        }
+    } else if (warp == 1) {
+        // ---- MMA issue (lane 0; the warp follows the loop) ----
+        unsigned g = 0;
+        int lt = 0;
+        for (int t = blockIdx.x; t < total; t += gridDim.x, lt++) {
+            int s, mt, nt;
+            wave_tile(sd, tstart, nsub, t, s, mt, nt);
+            const GemmDesc<T> &d = sd[s];
+            const int KT = ntiles(d.K, TL_K), bn = wave_tile_bn(d.N, nt);
+            const int set = lt % NSETS;
+            if (lt >= NSETS) wp_wait(smem_u32(tempty + set), ((lt / NSETS) - 1) & 1, vbad);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const unsigned acc = tmem + (unsigned)(set * Cfg::SET_COLS);
+            const int per = 256 / bn;   // B slices per MMA at most
+            const unsigned bstep = (unsigned)(NS * bn * I8_BK);   // one k tile of B slices
+            for (int k0 = 0; k0 < KT; k0 += KS, g++) {
+                const int ktn = KT - k0 < KS ? KT - k0 : KS;
+                const int buf = (int)(g % ST);
+                wp_wait(smem_u32(full + buf), (g / ST) & 1, vbad);
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                if (lane == 0) {
+                    const unsigned a0 = smem_u32(wpsm + buf * Cfg::STAGE);
+                    // descriptors of the stage's first A and B slices; a slice
+                    // or k tile further is an addition to the start-address field
+                    const uint64_t da0 = umma_desc(a0, 128, 256);
+                    const uint64_t db0 = umma_desc(a0 + KS * NS * I8_A_SLICE, 128, 512);
+                    for (int j = 0; j < ktn; j++) {
+#pragma unroll
+                    for (int i = 0; i < NS; i++) {
+                        const uint64_t da = da0 + (uint64_t)((j * NS + i) * (I8_A_SLICE >> 4));
+                        for (int j0 = 0; j0 < NS - i; j0 += per) {
+                            const int nb = (NS - i - j0) < per ? (NS - i - j0) : per;
+                            const uint64_t db = db0 + (uint64_t)((j * bstep + j0 * bn * I8_BK) >> 4);
+                            const unsigned dcol = acc + (unsigned)((i + j0) * bn);
+                            const unsigned en = (k0 > 0 || j > 0 || i > 0) ? 1u : 0u;
+                            asm volatile("{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+                                         "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, "
+                                         "{%5, %5, %5, %5}, p;\n}\n"
+                                         :: "r"(dcol), "l"(da), "l"(db), "r"(i8_idesc_n(nb * bn)),
+                                            "r"(en), "r"(0u)
+                                         : "memory");
+                        }
+                    }
+                    }
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                                 :: "r"(smem_u32(empty + buf)) : "memory");
+                    if (k0 + KS >= KT)
+                        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                                     :: "r"(smem_u32(tfull + set)) : "memory");
+                }
+                __syncwarp();
+            }
+        }
+    } else if (warp >= WP_EPI_WARP0) {
+        // ---- epilogue: warp e reads TMEM lanes 32 (e % 4) .. (tile rows) and
+        // the column half e / 4 of the tile into its shared-memory block (a
+        // lane per row), then stores the block along rows (pass `it` of a
+        // lane covers element it * 32 + lane of the 32 x cw block) ----
+        const int e = warp - WP_EPI_WARP0, rq = e & 3, ch = e >> 2;
+        T *blk = epi_stage + e * 32 * (CW + 1);
+        int lt = 0;
+        for (int t = blockIdx.x; t < total; t += gridDim.x, lt++) {
+            int s, mt, nt;
+            wave_tile(sd, tstart, nsub, t, s, mt, nt);
+            // register copies of the tile's descriptor and field output: the
+            // stores below could alias shared memory as far as the compiler
+            // knows, so references into shared memory would be reloaded
+            // after every store
+            const GemmDesc<T> &ds = sd[s];
+            EpiDesc<T> d;
+            d.C = ds.C; d.E = ds.E; d.ldc = ds.ldc; d.lde = ds.lde; d.rmul = ds.rmul; d.radd = ds.radd;
+            d.cmul = ds.cmul; d.cadd = ds.cadd; d.M = ds.M; d.N = ds.N;
+            const int prob = ds.prob;
+            const FieldOut o = so[prob];
+            const int ea = operand_exp(ds.amax_a), eb = operand_exp(ds.amax_b);
+            const int bn = wave_tile_bn(d.N, nt), cw = bn / 2;
+            const int r0 = mt * I8_BM + 32 * rq, n0 = nt * WP_BN + ch * cw;
+            const double scale = ldexp(1.0, ea + eb - 33);
+            const int set = lt % NSETS;
+            wp_wait(smem_u32(tfull + set), (lt / NSETS) & 1, vbad);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const unsigned acc = tmem + ((unsigned)(32 * rq) << 16) + (unsigned)(set * Cfg::SET_COLS);
+            const bool poison = *vbad != 0;
+#pragma unroll
+            for (int c8 = 0; c8 < CW / 8; c8++) {
+                if (8 * c8 >= cw) break;
+                unsigned r[NS][8];
+#pragma unroll
+                for (int q = 0; q < NS; q++) {
+                    const unsigned taddr = acc + (unsigned)(q * bn + ch * cw + 8 * c8);
+                    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                                 : "=r"(r[q][0]), "=r"(r[q][1]), "=r"(r[q][2]), "=r"(r[q][3]),
+                                   "=r"(r[q][4]), "=r"(r[q][5]), "=r"(r[q][6]), "=r"(r[q][7])
+                                 : "r"(taddr));
+                }
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int x = 0; x < 8; x++) {
+                    const long long c = ((long long)(int)r[0][x] << 21) + ((long long)(int)r[1][x] << 14) +
+                                        ((long long)(int)r[2][x] << 7) + (long long)(int)r[3][x];
+                    T v;
+                    if constexpr (NS == 4) {
+                        v = (T)((float)c * (float)scale);
+                    } else {
+                        const long long c2 = ((long long)(int)r[4][x] << 21) + ((long long)(int)r[5][x] << 14) +
+                                             ((long long)(int)r[6][x] << 7) + (long long)(int)r[7][x];
+                        v = (T)(((double)c + ldexp((double)c2, -28)) * scale);
+                    }
+                    blk[lane * (CW + 1) + 8 * c8 + x] = poison ? (T)__int_as_float(0x7fc00000) : v;
+                }
+            }
+            // the accumulators are in shared memory: release the set to the MMA warp
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(tempty + set));
+            // stores along rows, eight passes at a time: the eight operands
+            // the epilogue reads (spectral factors, previous fields) are
+            // loaded together first
+            double part = 0;
+            float vmax = 0.f;
+            for (int c0 = 0; c0 < cw; c0 += 8) {
+                double pre[8];
+#pragma unroll
+                for (int x = 0; x < 8; x++) {
+                    const int el = (c0 + x) * 32 + lane, row = el / cw, col = el - row * cw;
+                    pre[x] = (EPI != EPI_STORE && r0 + row < d.M && n0 + col < d.N)
+                                 ? epi_pre<EPI, T>(o, grid_n, d, r0 + row, n0 + col) : 0.0;
+                }
+#pragma unroll
+                for (int x = 0; x < 8; x++) {
+                    const int el = (c0 + x) * 32 + lane, row = el / cw, col = el - row * cw;
+                    if (r0 + row >= d.M || n0 + col >= d.N) continue;
+                    part += epi_apply<EPI, T>(o, grid_n, d, r0 + row, n0 + col, blk[row * (CW + 1) + col],
+                                              pre[x], vmax);
+                }
+            }
+            __syncwarp();   // the block is rewritten by the next tile
+            if (EPI != EPI_FIELD && amax_out) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+                if (lane == 0 && vmax > 0.f) atomicMax(amax_out + prob, __float_as_uint(vmax));
+            }
+            if (EPI == EPI_FIELD && o.kind == 3) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+                if (lane == 0) atomicAdd(o.bz_sum, part);
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(512) : "memory");
 }
 
 // ---------------------------------------------------------------------------
@@ -701,8 +1068,8 @@ struct FoldBatch {
 // consecutive elements along the contiguous direction of a core-matrix row
 // (K for A, N for B): one 32-bit store per plane.
 template <int NS, typename T>
-__device__ __forceinline__ void put_slices4(uint8_t *blk, int64_t plane, int64_t at,
-                                            const T v[4], double scale)
+__device__ __forceinline__ void put_slices4(uint8_t *blk, int64_t at, int stride, const T v[4],
+                                            double scale)
 {
     unsigned w[NS];
 #pragma unroll
@@ -715,7 +1082,7 @@ __device__ __forceinline__ void put_slices4(uint8_t *blk, int64_t plane, int64_t
         for (int i = 0; i < NS; i++) w[i] |= sl[i] << (8 * e);
     }
 #pragma unroll
-    for (int i = 0; i < NS; i++) *reinterpret_cast<unsigned *>(blk + i * plane + at) = w[i];
+    for (int i = 0; i < NS; i++) *reinterpret_cast<unsigned *>(blk + at + (int64_t)i * stride) = w[i];
 }
 
 // One thread per 32-bit word of every slice plane (four consecutive
@@ -758,9 +1125,9 @@ __global__ void __launch_bounds__(FOLD_THREADS) k_fold_slices(const __grid_const
             else if (!isv) v[e] = j < mid ? x[j] + x[C - 1 - j] : (j == mid ? x[mid] : T(0));
             else v[e] = j < ho ? x[j] - x[C - 1 - j] : T(0);
         }
-        if (!isv) put_slices4<NS>(blk, a_plane_bytes(R, he), a_tile_off(r, k, KTu), v, scale);
-        else put_slices4<NS>(blk + NS * a_plane_bytes(R, he), a_plane_bytes(R, ho),
-                             a_tile_off(r, k, KTv), v, scale);
+        if (!isv) put_slices4<NS>(blk, a_tile_off(r, k, KTu, NS, 0), I8_A_SLICE, v, scale);
+        else put_slices4<NS>(blk + NS * a_plane_bytes(R, he), a_tile_off(r, k, KTv, NS, 0), I8_A_SLICE,
+                             v, scale);
     } else {
         const int he = (R + 1) / 2, ho = R - he, mid = (R - 1) / 2;
         const int KTu = ntiles(he, TL_K), KTv = ntiles(ho, TL_K);
@@ -782,9 +1149,9 @@ __global__ void __launch_bounds__(FOLD_THREADS) k_fold_slices(const __grid_const
             const int c = n + e;
             v[e] = (!valid || c >= C) ? T(0) : (single ? ra[c] : (isv ? ra[c] - rb[c] : ra[c] + rb[c]));
         }
-        if (!isv) put_slices4<NS>(blk, b_plane_bytes(he, C), b_tile_off(k, n, KTu), v, scale);
-        else put_slices4<NS>(blk + NS * b_plane_bytes(he, C), b_plane_bytes(ho, C),
-                             b_tile_off(k, n, KTv), v, scale);
+        if (!isv) put_slices4<NS>(blk, b_tile_off(k, n, KTu, NS, 0), TL_K * TL_N, v, scale);
+        else put_slices4<NS>(blk + NS * b_plane_bytes(he, C), b_tile_off(k, n, KTv, NS, 0), TL_K * TL_N,
+                             v, scale);
     }
 }
 
@@ -1049,11 +1416,71 @@ static int launch_i8(const GemmBatch<T> &b, int nsub, int maxM, int maxN, cudaSt
     return LCB_OK;
 }
 
+template <typename T, int EPI, int KS>
+static int launch_wave_ks(GemmBatch<T> b, int nsub, cudaStream_t st)
+{
+    using Cfg = WPCfg<Slices<T>::n, KS>;
+    static std::atomic<unsigned long long> attr{0};
+    {
+        const cudaError_t e = ensure_smem(k_wave_i8p<T, EPI, KS>, Cfg::smem, attr);
+        if (e != cudaSuccess) return cuda_check(e, "persistent wave smem attribute");
+    }
+    b.nsub = nsub;
+    int total = 0;
+    for (int s = 0; s < nsub; s++) total += ntiles(b.d[s].M, I8_BM) * ntiles(b.d[s].N, WP_BN);
+    if (total == 0) return LCB_OK;
+    const int grid = total < sm_count() ? total : sm_count();
+    const cudaError_t e = launch_after(k_wave_i8p<T, EPI, KS>, dim3(grid), dim3(WP_THREADS), Cfg::smem,
+                                       st, b, total);
+    if (e != cudaSuccess) return cuda_check(e, "persistent wave launch");
+    return LCB_OK;
+}
+
+// k tiles per pipeline stage: LCB_WAVE_KS (1 or 2) if set, else 1 in FP64
+// (a 48 KB stage) and 2 in mixed precision (two 24 KB k tiles).
+static int wave_ks(int ns)
+{
+    static const int env = [] {
+        const char *v = getenv("LCB_WAVE_KS");
+        return v ? atoi(v) : 0;
+    }();
+    if (env == 1 || env == 2) return env;
+    return ns == 8 ? 1 : 2;
+}
+
+template <typename T, int EPI>
+static int launch_wave_p(const GemmBatch<T> &b, int nsub, cudaStream_t st)
+{
+    if constexpr (Slices<T>::n == 4)
+        if (wave_ks(4) == 2) return launch_wave_ks<T, EPI, 2>(b, nsub, st);
+    return launch_wave_ks<T, EPI, 1>(b, nsub, st);
+}
+
+// Which wave kernel runs: the persistent one for eight slices (FP64), the
+// one-tile-per-CTA kernel for four (mixed precision), where two CTAs per SM
+// overlap their epilogues and measured faster; LCB_WAVE_KERNEL=tiled or
+// =persistent selects one for both (read once per process).
+static bool persistent_waves(int ns)
+{
+    static const int mode = [] {
+        const char *v = getenv("LCB_WAVE_KERNEL");
+        if (v && strcmp(v, "tiled") == 0) return 1;
+        if (v && strcmp(v, "persistent") == 0) return 2;
+        return 0;
+    }();
+    return mode == 2 || (mode == 0 && ns == 8);
+}
+
 template <typename T>
 static int launch_wave(const GemmBatch<T> &b, int nsub, int epi, int maxM, int maxN,
                        int N, cudaStream_t st)
 {
     (void)N;
+    if (persistent_waves(Slices<T>::n)) {
+        if (epi == EPI_STORE) return launch_wave_p<T, EPI_STORE>(b, nsub, st);
+        if (epi == EPI_SCALE) return launch_wave_p<T, EPI_SCALE>(b, nsub, st);
+        return launch_wave_p<T, EPI_FIELD>(b, nsub, st);
+    }
     if (epi == EPI_STORE) return launch_i8<T, EPI_STORE>(b, nsub, maxM, maxN, st);
     if (epi == EPI_SCALE) return launch_i8<T, EPI_SCALE>(b, nsub, maxM, maxN, st);
     return launch_i8<T, EPI_FIELD>(b, nsub, maxM, maxN, st);
@@ -1189,8 +1616,6 @@ static int solve(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st
                     // tiled slice planes (A role): U block, then V block
                     const uint8_t *base = reinterpret_cast<const uint8_t *>(w.S2[p]);
                     d.A = reinterpret_cast<const T *>(base + (par ? Slices<T>::n * a_plane_bytes(rows[p], he) : 0));
-                    d.a_plane = (int)a_plane_bytes(rows[p], d.K);
-                    d.b_plane = (int)b_plane_bytes((int)L.rows[id], (int)L.cols[id]);
                 }
             }
         }
@@ -1219,8 +1644,6 @@ static int solve(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st
                     // tiled slice planes (B role): U block, then V block
                     const uint8_t *base = reinterpret_cast<const uint8_t *>(w.S2[p]);
                     d.B = reinterpret_cast<const T *>(base + (par ? Slices<T>::n * b_plane_bytes(he, cols[p]) : 0));
-                    d.b_plane = (int)b_plane_bytes(d.K, cols[p]);
-                    d.a_plane = (int)a_plane_bytes((int)L.rows[id], (int)L.cols[id]);
                 }
             }
         }

@@ -1,7 +1,8 @@
-"""Device-recorded diagnostics against the reference's FXiDiag / SliceDiag
-output files (tests/golden/diag_golden.npz, made by make_diag_golden.py from
-the same seeded inputs).  Runs on CPU tensors: the recording is device
-agnostic."""
+"""Device-recorded diagnostics against the reference's FXiDiag / SliceDiag /
+ParticlesDiag output files (tests/golden/diag_golden.npz, made by
+make_diag_golden.py from the same seeded inputs).  Runs on CPU tensors and,
+marked gpu, on CUDA tensors (the recording the drop-in Simulation does on
+the device)."""
 import os
 import sys
 import types
@@ -22,12 +23,19 @@ from lcodepy_b200.data import Arrays, DeviceArray  # noqa: E402
 GOLD = np.load(os.path.join(HERE, "golden", "diag_golden.npz"))
 
 
-def _ns(**kw):
-    return types.SimpleNamespace(**{k: DeviceArray(torch.as_tensor(v)) for k, v in kw.items()})
+def _ns(dev, **kw):
+    return types.SimpleNamespace(**{k: DeviceArray(torch.as_tensor(v, device=dev))
+                                    for k, v in kw.items()})
 
 
+DEVICES = ["cpu", pytest.param("cuda", marks=pytest.mark.gpu)]
+
+
+@pytest.mark.parametrize("dev", DEVICES)
 @pytest.mark.parametrize("case,cls,kw", CASES, ids=[c[0] for c in CASES])
-def test_diagnostic_files_match_reference(tmp_path, monkeypatch, case, cls, kw):
+def test_diagnostic_files_match_reference(tmp_path, monkeypatch, case, cls, kw, dev):
+    if dev == "cuda" and not torch.cuda.is_available():
+        pytest.skip("needs CUDA")
     monkeypatch.chdir(tmp_path)
     cfg = Config(dict(CONFIG))
     cfg._adjust_config_values_3d()
@@ -41,12 +49,13 @@ def test_diagnostic_files_match_reference(tmp_path, monkeypatch, case, cls, kw):
         if last_t is not None and t != last_t:
             d.dump(last_t, xi, particles, None, None, drain)
         last_t = t
-        fields = _ns(**{n: f[n] for n in ('Ex', 'Ey', 'Ez', 'Bx', 'By', 'Bz', 'Phi')})
-        currents = _ns(ro=f['ro'])
+        fields = _ns(dev, **{n: f[n] for n in ('Ex', 'Ey', 'Ez', 'Bx', 'By', 'Bz', 'Phi')})
+        currents = _ns(dev, ro=f['ro'])
         # what the drop-in Simulation hands to diagnostics: wrapped Arrays
-        particles = {'electrons': Arrays(torch, **{n: torch.as_tensor(f[n])
+        particles = {'electrons': Arrays(torch, **{n: torch.as_tensor(f[n], device=dev)
                                                    for n in ('m', 'px', 'py', 'pz')}).wrapped()}
-        d.after_step_dxi(t, xi, particles, fields, currents, DeviceArray(torch.as_tensor(f['rho_beam'])))
+        d.after_step_dxi(t, xi, particles, fields, currents,
+                         DeviceArray(torch.as_tensor(f['rho_beam'], device=dev)))
     d.dump(last_t, 0.0, particles, None, None, drain)
     sub = tmp_path / 'diagnostics' / kw['directory_name']
     want = sorted({k.split('|')[1] for k in GOLD.files if k.startswith(case + '|')})

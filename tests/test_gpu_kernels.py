@@ -378,15 +378,16 @@ def _plane_bytes(i, r, c):
     return _tiles(r, 32) * _tiles(c, 64) * 2048
 
 
-def _tile_offsets(i, r, c):
-    """Byte offset of every element (row, col) of a tiled slice plane."""
+def _tile_offsets(i, r, c, ns, k):
+    """Byte offset of slice k of every element (row, col) of a tiled block
+    (the ns slices of a tile are stored back to back)."""
     R, Cc = np.meshgrid(np.arange(r), np.arange(c), indexing="ij")
     if _a_role(i):
         KT = _tiles(c, 32)
-        return (((R >> 7) * KT + (Cc >> 5)) << 12) + ((R & 127) >> 3) * 256 + \
+        return ((((R >> 7) * KT + (Cc >> 5)) * ns + k) << 12) + ((R & 127) >> 3) * 256 + \
             ((Cc & 31) >> 4) * 128 + (R & 7) * 16 + (Cc & 15)
     KT = _tiles(r, 32)
-    return (((Cc >> 6) * KT + (R >> 5)) << 11) + ((Cc & 63) >> 4) * 512 + \
+    return ((((Cc >> 6) * KT + (R >> 5)) * ns + k) << 11) + ((Cc & 63) >> 4) * 512 + \
         ((R & 31) >> 3) * 128 + (R & 7) * 16 + (Cc & 15)
 
 
@@ -414,11 +415,10 @@ def test_field_operators_build(N, mixed):
     ns = 4 if mixed else 8          # slices per element = bytes per element
     for i, (ref, shp, off, ld) in enumerate(zip(blocks, shapes, offs, lds)):
         if i < 8:
-            # ns tiled int8 slice planes, x = 2 sum_k s_k 2^-(6 + 7 k)
+            # ns int8 slices per element in tiles, x = 2 sum_k s_k 2^-(6 + 7 k)
             plane = _plane_bytes(i, *shp)
-            at = _tile_offsets(i, *shp)
-            planes = [raw[ns * off + k * plane:ns * off + (k + 1) * plane].view(np.int8)[at]
-                      .astype(np.float64) for k in range(ns)]
+            blk = raw[ns * off:ns * off + ns * plane].view(np.int8)
+            planes = [blk[_tile_offsets(i, *shp, ns, k)].astype(np.float64) for k in range(ns)]
             got = 2 * sum(p * 2.0 ** -(6 + 7 * k) for k, p in enumerate(planes))
             # FP32 rounding of the value, then exact slices (mixed); FP64
             rel_b = 2.0 ** -23 if mixed else 1e-15

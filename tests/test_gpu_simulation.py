@@ -415,3 +415,24 @@ def test_mixed_precision_beam_energy():
     print(f"mixed vs FP64 beam: mean energy {e_mean:.2e}, energy change {e_change:.2e} "
           f"(FP64 change {m64 - e0:.3e} of {e0:.3f}), on-axis Ez {e_axis:.2e}")
     assert e_mean < 1e-5 and e_change < 1e-5 and e_axis < 1e-5
+
+
+def test_resume_matches_reference_resume(golden):
+    """A plasma state file written by plasma_state.save_plasmastate from the
+    reference's own run (after xi layer 56), resumed through the drop-in
+    Simulation with external_plasmastate, against the reference's Simulation
+    resuming from the same file (tests/golden/make_resume_golden.py)."""
+    import os
+    ref = golden("run_resume.npz")
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "resume_state.npz")
+    sim = Simulation(config=cfg(**{'rigid-beam': True, 'window-length': 4.0}),
+                     beam_parameters=rigid_driver, runas_filename='')
+    sim.external_plasmastate = True
+    sim.path_to_plasmastate = path
+    sim.step(1)
+    ps = sim.push_solver
+    particles, fields, currents = ps._plasmastate
+    ez = ps.ez_axis.cpu().numpy()
+    assert ez.shape == ref["ez_axis"].shape
+    assert rel_err(ez, ref["ez_axis"]) < 1e-8
+    check(ref, particles, fields, currents, ["electrons"], 1e-8)

@@ -6,8 +6,10 @@ inside liblcb.so.
 
 Checked through the C ABI against lcb_compute_fields with a caller workspace,
 on two calls in a row (the second call finds the first call's data in the
-shared array), at the tolerance the other compute_fields tests use.  Kept in
-a file of its own, collected last."""
+shared array), in FP64 and in mixed precision, up to the largest grid whose
+scratch fits the array (283 and 427), at the tolerances the other
+compute_fields tests use; grids beyond the array are rejected.  Kept in a
+file of its own, collected last."""
 import ctypes as C
 
 import numpy as np
