@@ -178,9 +178,20 @@ typedef struct lcb_compute_fields_args {
  * calculate_Ex_Ey_Bx_By :176-230, calculate_Ez :112-139, calculate_Bz
  * :233-266, calculate_Phi :142-159 and the GPU transforms :36-107): every
  * DST-I / DCT-I / mixed transform is a dense batched matrix product.
- * Phi is skipped when both its out_full and out_half planes are NULL. */
+ * Phi is skipped when both its out_full and out_half planes are NULL.
+ * The transforms run on one of two tensor-core wave kernels (one CTA per
+ * output tile, or a persistent warp-specialised one); the first call for a
+ * (device, grid_steps, precision) that is not under stream capture times
+ * both on the caller's stream and keeps the faster (it computes the same
+ * outputs several times and synchronises the stream once).
+ * LCB_WAVE_KERNEL=tiled or =persistent in the environment fixes the choice. */
 int lcb_compute_fields(const lcb_compute_fields_args *a, void *stream);
 size_t lcb_compute_fields_workspace_bytes(int grid_steps, int precision);
+
+/* The wave kernel chosen for (grid_steps, precision) on the current device:
+ * 1 one CTA per tile, 2 persistent, 0 not measured yet.  No counterpart in
+ * the reference (reporting only). */
+int lcb_wave_kernel_choice(int grid_steps, int precision);
 
 /* Allocation-free compute_fields.  No counterpart in the reference: it exists
  * for callers that cannot allocate device memory themselves -- a host code

@@ -100,6 +100,7 @@ _SIGS = {
     "lcb_compute_fields": (_i, [C.POINTER(ComputeFieldsArgs), _vp]),
     "lcb_compute_fields_workspace_bytes": (C.c_size_t, [_i, _i]),
     "lcb_compute_fields_noalloc": (_i, [C.POINTER(ComputeFieldsArgs), _vp]),
+    "lcb_wave_kernel_choice": (_i, [_i, _i]),
     "lcb_beam_deposit": (_i, [_i64, _i, _d, _d, _i64] + [_vp] * 6 + [_vp, _vp]),
     "lcb_beam_substepping": (_i, [_i64, _vp, _vp, _d, _d, _vp, _vp, _vp]),
     "lcb_beam_step": (_i, [C.POINTER(BeamStepArgs), _vp]),

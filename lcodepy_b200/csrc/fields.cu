@@ -492,6 +492,13 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
     unsigned *tslot = reinterpret_cast<unsigned *>(fin + 1);
 
     const GemmDesc<T> &g = batch.d[blockIdx.z];
+    // register copies of what the epilogue reads (parameter reads indexed by
+    // blockIdx.z are slow)
+    EpiDesc<T> ge;
+    ge.C = g.C; ge.E = g.E; ge.ldc = g.ldc; ge.lde = g.lde; ge.rmul = g.rmul; ge.radd = g.radd;
+    ge.cmul = g.cmul; ge.cadd = g.cadd; ge.M = g.M; ge.N = g.N;
+    const FieldOut go = batch.out[g.prob];
+    const int grid_n = batch.grid_n;
     const int M = g.M, N = g.N, K = g.K;
     const int m0 = blockIdx.y * I8_BM, n0 = blockIdx.x * BN;
     if (m0 >= M || n0 >= N) return;
@@ -571,7 +578,7 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
         const int e = it * 32 + lane, row = e / CW, col = e % CW;
         const int gm = m0 + 32 * rq + row, gn = n0 + CW * ch + col;
         pre[it] = (EPI != EPI_STORE && gm < M && gn < N)
-                      ? epi_pre<EPI, T>(batch.out[g.prob], batch.grid_n, g, gm, gn) : 0.0;
+                      ? epi_pre<EPI, T>(go, grid_n, ge, gm, gn) : 0.0;
     }
 
     bool ok = true;
@@ -663,7 +670,7 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
         const int e = it * 32 + lane, row = e / CW, col = e % CW;
         const int gm = m0 + 32 * rq + row, gn = n0 + CW * ch + col;
         if (gm >= M || gn >= N) continue;
-        part += epi_apply<EPI, T>(batch.out[g.prob], batch.grid_n, g, gm, gn, stage[row * (CW + 1) + col],
+        part += epi_apply<EPI, T>(go, grid_n, ge, gm, gn, stage[row * (CW + 1) + col],
                                   pre[it], vmax);
     }
     if (EPI != EPI_FIELD && batch.amax_out) {
@@ -676,7 +683,7 @@ k_gemm_i8(const __grid_constant__ GemmBatch<T> batch)
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
                      :: "r"(tmem), "r"(Cfg::TMEM_COLS) : "memory");
-    if (EPI == EPI_FIELD && batch.out[g.prob].kind == 3) bz_reduce<Cfg::THREADS>(part, batch.out[g.prob].bz_sum);
+    if (EPI == EPI_FIELD && go.kind == 3) bz_reduce<Cfg::THREADS>(part, go.bz_sum);
 }
 
 // ---------------------------------------------------------------------------
@@ -1027,7 +1034,7 @@ k_wave_i8p(const __grid_constant__ GemmBatch<T> batch, int total)
             }
             if (EPI == EPI_FIELD && o.kind == 3) {
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+                for (int sh = 16; sh > 0; sh >>= 1) part += __shfl_xor_sync(0xffffffffu, part, sh);
                 if (lane == 0) atomicAdd(o.bz_sum, part);
             }
         }
@@ -1456,27 +1463,16 @@ static int launch_wave_p(const GemmBatch<T> &b, int nsub, cudaStream_t st)
     return launch_wave_ks<T, EPI, 1>(b, nsub, st);
 }
 
-// Which wave kernel runs: the persistent one for eight slices (FP64), the
-// one-tile-per-CTA kernel for four (mixed precision), where two CTAs per SM
-// overlap their epilogues and measured faster; LCB_WAVE_KERNEL=tiled or
-// =persistent selects one for both (read once per process).
-static bool persistent_waves(int ns)
-{
-    static const int mode = [] {
-        const char *v = getenv("LCB_WAVE_KERNEL");
-        if (v && strcmp(v, "tiled") == 0) return 1;
-        if (v && strcmp(v, "persistent") == 0) return 2;
-        return 0;
-    }();
-    return mode == 2 || (mode == 0 && ns == 8);
-}
+// The two forms of the transform waves: one CTA per output tile, or the
+// persistent warp-specialised kernel.  Which one runs for a grid and
+// precision is measured (wave_kernel_for below).
+enum { WK_TILED = 1, WK_PERSISTENT = 2 };
 
 template <typename T>
 static int launch_wave(const GemmBatch<T> &b, int nsub, int epi, int maxM, int maxN,
-                       int N, cudaStream_t st)
+                       int wk, cudaStream_t st)
 {
-    (void)N;
-    if (persistent_waves(Slices<T>::n)) {
+    if (wk == WK_PERSISTENT) {
         if (epi == EPI_STORE) return launch_wave_p<T, EPI_STORE>(b, nsub, st);
         if (epi == EPI_SCALE) return launch_wave_p<T, EPI_SCALE>(b, nsub, st);
         return launch_wave_p<T, EPI_FIELD>(b, nsub, st);
@@ -1487,7 +1483,7 @@ static int launch_wave(const GemmBatch<T> &b, int nsub, int epi, int maxM, int m
 }
 
 template <typename T>
-static int run_wave(const GemmBatch<T> &b, int nsub, int epi, int N, cudaStream_t st,
+static int run_wave(const GemmBatch<T> &b, int nsub, int epi, int wk, cudaStream_t st,
                     const char *what)
 {
     int maxM = 0, maxN = 0;
@@ -1495,7 +1491,7 @@ static int run_wave(const GemmBatch<T> &b, int nsub, int epi, int N, cudaStream_
         maxM = b.d[s].M > maxM ? b.d[s].M : maxM;
         maxN = b.d[s].N > maxN ? b.d[s].N : maxN;
     }
-    const int rc = launch_wave(b, nsub, epi, maxM, maxN, N, st);
+    const int rc = launch_wave(b, nsub, epi, maxM, maxN, wk, st);
     if (rc) return rc;
     LCB_LAUNCH_CHECK(what);
     return LCB_OK;
@@ -1533,7 +1529,7 @@ static int run_fold(T *const *src, T *const *dst, const int *probs, int np, cons
 }
 
 template <typename T>
-static int solve(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st)
+static int solve(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st, int wk)
 {
     const int N = a->grid_steps, n = N - 2;
     const OpLayout L = op_layout(N);
@@ -1655,17 +1651,17 @@ static int solve(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st
     if ((rc = run_fold<T>(w.S1, w.S2, probs, np, rows, cols, 0, N, st, mx0, mx1))) return rc;
     cur_mx = mx0;
     b.amax_out = mx1;
-    if ((rc = run_wave<T>(b, right_wave(), EPI_STORE, N, st, "wave1"))) return rc;
+    if ((rc = run_wave<T>(b, right_wave(), EPI_STORE, wk, st, "wave1"))) return rc;
     // wave 2: S1 = (L S1) o Mat
     if ((rc = run_fold<T>(w.S1, w.S2, probs, np, rows, cols, 1, N, st, mx1, mx0))) return rc;
     cur_mx = mx1;
     b.amax_out = mx0;
-    if ((rc = run_wave<T>(b, left_wave(false), EPI_SCALE, N, st, "wave2"))) return rc;
+    if ((rc = run_wave<T>(b, left_wave(false), EPI_SCALE, wk, st, "wave2"))) return rc;
     // wave 3: S1 = S1 R
     if ((rc = run_fold<T>(w.S1, w.S2, probs, np, rows, cols, 0, N, st, mx0, mx1))) return rc;
     cur_mx = mx0;
     b.amax_out = mx1;
-    if ((rc = run_wave<T>(b, right_wave(), EPI_STORE, N, st, "wave3"))) return rc;
+    if ((rc = run_wave<T>(b, right_wave(), EPI_STORE, wk, st, "wave3"))) return rc;
     // wave 4: fields = L S1
     if ((rc = run_fold<T>(w.S1, w.S2, probs, np, rows, cols, 1, N, st, mx1, mx0))) return rc;
     cur_mx = mx1;
@@ -1684,7 +1680,7 @@ static int solve(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st
         o.row_off = roff[p]; o.col_off = coff[p]; o.kind = kind[p];
         o.bz_raw = w.bz_raw; o.bz_sum = w.bz_sum;
     }
-    if ((rc = run_wave<T>(b, nsub, EPI_FIELD, N, st, "wave4"))) return rc;
+    if ((rc = run_wave<T>(b, nsub, EPI_FIELD, wk, st, "wave4"))) return rc;
 
     FinishArgs fa;
     fa.N = N; fa.bz_raw = w.bz_raw; fa.bz_sum = w.bz_sum;
@@ -1755,6 +1751,98 @@ extern "C" size_t lcb_compute_fields_workspace_bytes(int grid_steps, int precisi
                                        : work_bytes<double>(grid_steps);
 }
 
+// ---------------------------------------------------------------------------
+// Wave-kernel autotuner.  The first compute_fields of a (device, grid,
+// precision) that is not being captured into a graph times the solve with
+// each wave kernel (two warm-up and three timed calls each, CUDA events on
+// the caller's stream) and keeps the faster; calls under capture before that
+// use the one that measured faster on B200 at N = 513 (persistent for FP64,
+// one tile per CTA for mixed precision).  The tuning calls compute the same
+// outputs as the call itself (compute_fields only reads its inputs), so the
+// call's result is unchanged.  LCB_WAVE_KERNEL=tiled or =persistent fixes the
+// choice for every grid.
+// ---------------------------------------------------------------------------
+#include <map>
+#include <mutex>
+#include <tuple>
+
+namespace lcb {
+
+static std::mutex g_tune_mu;
+static std::map<std::tuple<int, int, int>, int> g_tuned;   // (device, N, precision) -> WK_*
+
+static int wave_kernel_env()
+{
+    static const int mode = [] {
+        const char *v = getenv("LCB_WAVE_KERNEL");
+        if (v && strcmp(v, "tiled") == 0) return (int)WK_TILED;
+        if (v && strcmp(v, "persistent") == 0) return (int)WK_PERSISTENT;
+        return 0;
+    }();
+    return mode;
+}
+
+template <typename T>
+static int solve_tuned(const lcb_compute_fields_args *a, const T *ops, cudaStream_t st)
+{
+    const int fixed = wave_kernel_env();
+    if (fixed) return solve<T>(a, ops, st, fixed);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_check(e, "cudaGetDevice");
+    const auto key = std::make_tuple(dev, a->grid_steps, a->precision);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) return solve<T>(a, ops, st, it->second);
+    }
+    const int fallback = Slices<T>::n == 8 ? WK_PERSISTENT : WK_TILED;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(st, &cs);
+    if (e != cudaSuccess) return cuda_check(e, "cudaStreamIsCapturing");
+    if (cs != cudaStreamCaptureStatusNone) return solve<T>(a, ops, st, fallback);
+    cudaEvent_t ev[2];
+    if ((e = cudaEventCreate(&ev[0])) != cudaSuccess) return cuda_check(e, "tuner event");
+    if ((e = cudaEventCreate(&ev[1])) != cudaSuccess) {
+        cudaEventDestroy(ev[0]);
+        return cuda_check(e, "tuner event");
+    }
+    const int cand[2] = {WK_TILED, WK_PERSISTENT};
+    float best = 0.f;
+    int pick = fallback, rc = LCB_OK;
+    for (int c = 0; c < 2 && rc == LCB_OK; c++) {
+        for (int r = 0; r < 2 && rc == LCB_OK; r++) rc = solve<T>(a, ops, st, cand[c]);
+        if (rc) break;
+        cudaEventRecord(ev[0], st);
+        for (int r = 0; r < 3 && rc == LCB_OK; r++) rc = solve<T>(a, ops, st, cand[c]);
+        cudaEventRecord(ev[1], st);
+        if (rc) break;
+        if ((e = cudaEventSynchronize(ev[1])) != cudaSuccess) { rc = cuda_check(e, "tuner sync"); break; }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[0], ev[1]);
+        if (c == 0 || ms < best) { best = ms; pick = cand[c]; }
+    }
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    if (rc) return rc;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tuned[key] = pick;
+    }
+    return solve<T>(a, ops, st, pick);
+}
+
+}  // namespace lcb
+
+extern "C" int lcb_wave_kernel_choice(int grid_steps, int precision)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    std::lock_guard<std::mutex> lock(lcb::g_tune_mu);
+    auto it = lcb::g_tuned.find(std::make_tuple(dev, grid_steps, precision));
+    return it == lcb::g_tuned.end() ? 0 : it->second;
+}
+
 extern "C" int lcb_compute_fields(const lcb_compute_fields_args *a, void *stream)
 {
     LCB_REQUIRE(a, "args is NULL");
@@ -1774,9 +1862,9 @@ extern "C" int lcb_compute_fields(const lcb_compute_fields_args *a, void *stream
     for (int f = 0; f < 6; f++) LCB_REQUIRE(a->fields_prev.f[f], "fields_prev plane %d is NULL", f);
     cudaStream_t st = as_stream(stream);
     if (a->precision == LCB_PREC_MIXED)
-        return solve<float>(a, static_cast<const float *>(a->operators), st);
+        return solve_tuned<float>(a, static_cast<const float *>(a->operators), st);
     LCB_REQUIRE(a->precision == LCB_PREC_FP64, "bad precision %d", a->precision);
-    return solve<double>(a, static_cast<const double *>(a->operators), st);
+    return solve_tuned<double>(a, static_cast<const double *>(a->operators), st);
 }
 
 // ---------------------------------------------------------------------------
