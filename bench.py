@@ -449,15 +449,17 @@ def run_serve(args, ws, rank, local):
     plain_value = cell_steps / finish
     # accuracy: a few requests rerun alone through the plain FP64 path
     # accuracy: every served result against the same request alone in FP64
-    errs = [float(np.linalg.norm(done[rid]["ez"] - plain[rid]["ez"]) /
-                  max(np.linalg.norm(plain[rid]["ez"]), 1e-300)) for rid in plain]
+    err_of = {rid: float(np.linalg.norm(done[rid]["ez"] - plain[rid]["ez"]) /
+                         max(np.linalg.norm(plain[rid]["ez"]), 1e-300)) for rid in plain}
+    errs = list(err_of.values())
+    worst = sorted(err_of.items(), key=lambda kv: -kv[1])[:3]
     return {"value": value, "ms": ms, "wall_s": wall, "cell_steps": cell_steps,
             "p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
             "plain_value": plain_value, "plain_p50": float(np.percentile(plain_lat, 50)),
             "plain_p99": float(np.percentile(plain_lat, 99)),
             "plain_busy_s": sum(v["seconds"] for v in plain.values()), "failed": failed,
             "beam_requests": sum(isinstance(r[3], BeamDriver) for r in reqs),
-            "errs": errs, "clocks": clocks, "launches": launches,
+            "errs": errs, "worst": worst, "clocks": clocks, "launches": launches,
             "span_arrivals_s": reqs[-1][0]}
 
 
@@ -533,7 +535,9 @@ def run_headline(args, ws, rank, local):
                                   "from the arrivals and the measured durations"},
             "served_vs_plain": v["value"] / v["plain_value"],
             "ez_rel_l2_vs_fp64": {"max": max(v["errs"]) if v["errs"] else None,
-                                  "median": float(np.median(v["errs"])) if v["errs"] else None},
+                                  "median": float(np.median(v["errs"])) if v["errs"] else None,
+                                  "over_1e-5": int(sum(e > 1e-5 for e in v["errs"])),
+                                  "worst": v["worst"]},
             "failed_requests": v["failed"], "gpu_launches": v["launches"],
             "clocks": v["clocks"]}
     except Exception as e:

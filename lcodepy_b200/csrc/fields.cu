@@ -86,6 +86,37 @@ __device__ __forceinline__ void slices_of<8>(double x, double scale, unsigned sl
     }
 }
 
+// The data operands' slices come from one float-to-integer conversion:
+// X = round(x * scale * 2^(6 + 7 (NS - 1))), the value x * scale rounded to
+// the last slice's unit as slices_of rounds it.  Its balanced base-128
+// digits (|s| <= 64, the top one may reach 64) are the unsigned 7-bit fields
+// of B = X + 64 (1 + 2^7 + ... + 2^(7 (NS - 1))) less 64 each; the fields
+// are returned with the 64 still added (0 .. 128), and put_slices4 removes
+// it from four packed bytes at once.
+__device__ __forceinline__ void slices_biased(double x, double scale, unsigned sl[8])
+{
+    const long long X = __double2ll_rn(x * scale * 36028797018963968.0);   // 2^55
+    const unsigned long long B = (unsigned long long)X + 0x81020408102040ull;
+    const unsigned lo = (unsigned)B, hi = (unsigned)(B >> 32);
+    sl[7] = lo & 127u;
+    sl[6] = (lo >> 7) & 127u;
+    sl[5] = (lo >> 14) & 127u;
+    sl[4] = (lo >> 21) & 127u;
+    sl[3] = __funnelshift_r(lo, hi, 28) & 127u;
+    sl[2] = (hi >> 3) & 127u;
+    sl[1] = (hi >> 10) & 127u;
+    sl[0] = hi >> 17;
+}
+__device__ __forceinline__ void slices_biased(float x, double scale, unsigned sl[4])
+{
+    const int X = __float2int_rn(x * (float)scale * 134217728.0f);          // 2^27
+    const unsigned B = (unsigned)X + 0x8102040u;
+    sl[3] = B & 127u;
+    sl[2] = (B >> 7) & 127u;
+    sl[1] = (B >> 14) & 127u;
+    sl[0] = B >> 21;
+}
+
 // Slices per element of an operand of type T (one byte each: the sliced
 // form takes the same storage as T).
 template <typename T> struct Slices { static constexpr int n = (int)sizeof(T); };
@@ -723,14 +754,17 @@ struct WPCfg {
     static constexpr int B_TILE = I8_BK * WP_BN;               // bytes per B slice (64 wide)
     static constexpr int KSTAGE = NS * (I8_A_SLICE + B_TILE);  // one k tile: 24 KB (4 slices) / 48 KB (8)
     static constexpr int STAGE = KS * KSTAGE;
-    static constexpr int ST = (144 * 1024) / STAGE;            // pipeline stages
-    static_assert(ST >= 2, "at least two pipeline stages");
     static constexpr int SET_COLS = NS * WP_BN;                // 256 / 512 TMEM columns
     static constexpr int NSETS = 512 / SET_COLS;               // 2 / 1 accumulator sets
     static constexpr int CW = WP_BN / 2;                       // epilogue columns per warp (max)
-    // per epilogue warp a 32 x CW block of outputs (one padding column), so
-    // that the stores run along rows
-    static constexpr int EPI_BYTES = WP_EPI_WARPS * 32 * (CW + 1) * NS;
+    // Per epilogue warp a 32 x CW block of outputs in shared memory (one
+    // padding column), so that the stores run along rows.  (Storing straight
+    // from registers, a lane per row, to make room for a fourth 48 KB FP64
+    // stage measured 4 % slower at N = 513.)
+    static constexpr bool STAGED = true;
+    static constexpr int EPI_BYTES = STAGED ? WP_EPI_WARPS * 32 * (CW + 1) * NS : 0;
+    static constexpr int ST = ((STAGED ? 144 : 192) * 1024) / STAGE;  // pipeline stages
+    static_assert(ST >= 2, "at least two pipeline stages");
     static constexpr size_t smem = (size_t)ST * STAGE + EPI_BYTES + 256;
 };
 
@@ -973,6 +1007,7 @@ k_wave_i8p(const __grid_constant__ GemmBatch<T> batch, int total)
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const unsigned acc = tmem + ((unsigned)(32 * rq) << 16) + (unsigned)(set * Cfg::SET_COLS);
             const bool poison = *vbad != 0;
+            T vreg[Cfg::STAGED ? 1 : CW];
 #pragma unroll
             for (int c8 = 0; c8 < CW / 8; c8++) {
                 if (8 * c8 >= cw) break;
@@ -998,19 +1033,40 @@ k_wave_i8p(const __grid_constant__ GemmBatch<T> batch, int total)
                                              ((long long)(int)r[6][x] << 7) + (long long)(int)r[7][x];
                         v = (T)(((double)c + ldexp((double)c2, -28)) * scale);
                     }
-                    blk[lane * (CW + 1) + 8 * c8 + x] = poison ? (T)__int_as_float(0x7fc00000) : v;
+                    if (poison) v = (T)__int_as_float(0x7fc00000);
+                    if constexpr (Cfg::STAGED) blk[lane * (CW + 1) + 8 * c8 + x] = v;
+                    else vreg[8 * c8 + x] = v;
                 }
             }
-            // the accumulators are in shared memory: release the set to the MMA warp
+            // the accumulators are in shared memory or registers: release the
+            // set to the MMA warp
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(tempty + set));
+            double part = 0;
+            float vmax = 0.f;
+            if constexpr (!Cfg::STAGED) {
+                // a lane stores its row, eight columns at a time
+                const int gm = r0 + lane;
+#pragma unroll
+                for (int c0 = 0; c0 < CW; c0 += 8) {
+                    if (c0 >= cw) break;
+                    double pre[8];
+#pragma unroll
+                    for (int x = 0; x < 8; x++)
+                        pre[x] = (EPI != EPI_STORE && gm < d.M && n0 + c0 + x < d.N)
+                                     ? epi_pre<EPI, T>(o, grid_n, d, gm, n0 + c0 + x) : 0.0;
+#pragma unroll
+                    for (int x = 0; x < 8; x++) {
+                        if (gm >= d.M || n0 + c0 + x >= d.N) continue;
+                        part += epi_apply<EPI, T>(o, grid_n, d, gm, n0 + c0 + x, vreg[c0 + x], pre[x], vmax);
+                    }
+                }
+            }
             // stores along rows, eight passes at a time: the eight operands
             // the epilogue reads (spectral factors, previous fields) are
             // loaded together first
-            double part = 0;
-            float vmax = 0.f;
-            for (int c0 = 0; c0 < cw; c0 += 8) {
+            for (int c0 = 0; Cfg::STAGED && c0 < cw; c0 += 8) {
                 double pre[8];
 #pragma unroll
                 for (int x = 0; x < 8; x++) {
@@ -1084,12 +1140,13 @@ __device__ __forceinline__ void put_slices4(uint8_t *blk, int64_t at, int stride
 #pragma unroll
     for (int e = 0; e < 4; e++) {
         unsigned sl[NS];
-        slices_of<NS>((double)v[e], scale, sl);
+        slices_biased(v[e], scale, sl);
 #pragma unroll
         for (int i = 0; i < NS; i++) w[i] |= sl[i] << (8 * e);
     }
 #pragma unroll
-    for (int i = 0; i < NS; i++) *reinterpret_cast<unsigned *>(blk + at + (int64_t)i * stride) = w[i];
+    for (int i = 0; i < NS; i++)
+        *reinterpret_cast<unsigned *>(blk + at + (int64_t)i * stride) = __vsub4(w[i], 0x40404040u);
 }
 
 // One thread per 32-bit word of every slice plane (four consecutive
