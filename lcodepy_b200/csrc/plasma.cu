@@ -686,14 +686,26 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
     }
 
     for (int t = threadIdx.x; t < 4 * WSZ; t += blockDim.x) sw[t] = Acc(0);
-    for (int t = threadIdx.x; t < WSZ; t += blockDim.x) {
-        const int gx = wx0 + t / WY, gy = wy0 + t % WY;
-        const bool in = gx >= 0 && gx < N && gy >= 0 && gy < N;
-        const int64_t g = (int64_t)gx * N + gy;
-        FT v[6];
+    // the field window, FILL_BATCH cells per thread at a time: the batch's
+    // loads are all in flight before the first store to the window
+    constexpr int FILL_ITERS = (WSZ + DEP_THREADS - 1) / DEP_THREADS, FILL_BATCH = 3;
 #pragma unroll
-        for (int f = 0; f < 6; f++) v[f] = in ? (FT)__ldg(fld[f] + g) : FT(0);
-        FieldWin<FT>::put(sf, WSZ, t, v);
+    for (int k0 = 0; k0 < FILL_ITERS; k0 += FILL_BATCH) {
+        FT v[FILL_BATCH][6];
+#pragma unroll
+        for (int k = 0; k < FILL_BATCH; k++) {
+            const int t = threadIdx.x + (k0 + k) * DEP_THREADS;
+            const int gx = wx0 + t / WY, gy = wy0 + t % WY;
+            const bool in = k0 + k < FILL_ITERS && t < WSZ && gx >= 0 && gx < N && gy >= 0 && gy < N;
+            const int64_t g = (int64_t)gx * N + gy;
+#pragma unroll
+            for (int f = 0; f < 6; f++) v[k][f] = in ? (FT)__ldg(fld[f] + g) : FT(0);
+        }
+#pragma unroll
+        for (int k = 0; k < FILL_BATCH; k++) {
+            const int t = threadIdx.x + (k0 + k) * DEP_THREADS;
+            if (k0 + k < FILL_ITERS && t < WSZ) FieldWin<FT>::put(sf, WSZ, t, v[k]);
+        }
     }
     __syncthreads();
 
@@ -745,10 +757,8 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
             if (err) atomicOr(err, LCB_DEVERR_PLASMA_STENCIL);
             ix[p] = -1000;  // no gather: zero fields, as in the reference's skip
         }
-        // FP64: the push's mass and momenta, loaded while the gather runs
-        // (in mixed precision the registers they would hold cost more spills
-        // than the early loads save)
-        if (!FIRST && !MIXED) { L_m[p] = m_a[k]; L_px[p] = px_p[k]; L_py[p] = py_p[k]; L_pz[p] = pz_p[k]; }
+        // the push's mass and momenta, loaded while the gather runs
+        if (!FIRST) { L_m[p] = m_a[k]; L_px[p] = px_p[k]; L_py[p] = py_p[k]; L_pz[p] = pz_p[k]; }
     }
 
     // ---- phase 2: gather ----
@@ -826,7 +836,6 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
         const int64_t k = kk[p];
         const FT *Fp = p ? F1 : F0;
         const double Ex = Fp[0], Ey = Fp[1], Ez = Fp[2], Bx = Fp[3], By = Fp[4], Bz = Fp[5];
-        if (!FIRST && MIXED) { L_m[p] = m_a[k]; L_px[p] = px_p[k]; L_py[p] = py_p[k]; L_pz[p] = pz_p[k]; }
         const double mk = L_m[p], qk = L_q[p];
         const double opx = L_px[p], opy = L_py[p], opz = L_pz[p];
         const double xi0 = x_init[k], yi0 = y_init[k];
