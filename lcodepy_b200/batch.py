@@ -372,20 +372,97 @@ def solo_ez(config: dict, driver, **overrides) -> np.ndarray:
 
 
 class BatchRunner:
-    """Advance a fixed set of members together, one xi step at a time."""
+    """Advance a fixed set of members together, one xi step at a time.
 
-    def __init__(self, members):
+    With ``single_graph`` (rigid-driver members of one length, advancing in
+    lockstep) every batched xi step after the members' two eager steps is ONE
+    graph launch: the members' steps are captured together, each on its own
+    stream forked from and joined back into the capturing stream, once per
+    buffer parity; otherwise each member replays its own graph on its
+    stream."""
+
+    MARK_EVERY = 16
+    MAX_AHEAD = 4
+
+    def __init__(self, members, single_graph=False):
         self.members = list(members)
+        self.single_graph = single_graph and len(self.members) > 0 and all(
+            type(m) is Member for m in self.members) and len(
+            {m.n_steps for m in self.members}) == 1
+        self.graphs = [None, None]
+        self.stream = torch.cuda.Stream(self.members[0].device) if self.single_graph else None
+        self.marks = collections.deque()
+        self.launches = 0
+
+    def _capture(self):
+        """One graph holding every member's xi step for the current parity."""
+        g = torch.cuda.CUDAGraph()
+        n0 = _lib.load().lcb_launch_count()
+        with torch.cuda.stream(self.stream):
+            g.capture_begin(capture_error_mode="thread_local")
+            try:
+                fork = torch.cuda.Event()
+                fork.record(self.stream)
+                for m in self.members:
+                    m.stream.wait_event(fork)
+                    with torch.cuda.stream(m.stream):
+                        m._ops()
+                    join = torch.cuda.Event()
+                    join.record(m.stream)
+                    self.stream.wait_event(join)
+            finally:
+                g.capture_end()
+        return g, _lib.load().lcb_launch_count() - n0
 
     def step(self):
+        if not self.single_graph or any(m.eager < 2 for m in self.members):
+            for m in self.members:
+                if not m.finished:
+                    m.step()
+            return
+        if self.members[0].finished:
+            return
+        p = self.members[0].solver.cur
+        if len(self.marks) >= self.MAX_AHEAD:
+            self.marks.popleft().synchronize()
+        if self.graphs[p] is None:
+            # the members' streams have work queued from their eager steps
+            for m in self.members:
+                self.stream.wait_stream(m.stream)
+            self.graphs[p] = self._capture()
+        g, nl = self.graphs[p]
+        # members' earlier work (eager steps) precedes the batch graph
         for m in self.members:
-            if not m.finished:
-                m.step()
+            self.stream.wait_stream(m.stream)
+        with torch.cuda.stream(self.stream):
+            g.replay()
+        _lib.add_replayed(nl)
+        for m in self.members:
+            ps = m.solver
+            m.done += 1
+            ps.cur = 1 - p
+            ps.last_fields = ps.fields[p]
+            if m.done >= m.n_steps:
+                ev = torch.cuda.Event()
+                ev.record(self.stream)
+                m.end_event = ev
+        if self.members[0].done % self.MARK_EVERY == 0:
+            ev = torch.cuda.Event()
+            ev.record(self.stream)
+            self.marks.append(ev)
+
+    def join(self):
+        """Make the members' streams wait for the batch graphs (before reading
+        results on a member's stream)."""
+        if self.single_graph:
+            for m in self.members:
+                m.stream.wait_stream(self.stream)
 
     def run(self, steps=None):
         n = steps if steps is not None else max(m.n_steps for m in self.members)
         for _ in range(n):
             self.step()
+        self.join()
         torch.cuda.synchronize()
 
     @property

@@ -31,6 +31,24 @@ def rel(a, b):
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
 
 
+def test_single_graph_batch_equals_solo_runs():
+    """Every member's xi step captured into one graph per buffer parity (one
+    graph launch per batched xi step): each member equals its solo run."""
+    specs = [(cfg(1.6, 30), GaussianDriver(0.3, 0.8)),
+             (cfg(3.25, 30, precision="mixed"), GaussianDriver(0.05, 1.5)),
+             (cfg(1.6, 30), GaussianDriver(0.5, 0.6))]
+    members = [Member(c, d) for c, d in specs]
+    runner = BatchRunner(members, single_graph=True)
+    assert runner.single_graph
+    runner.run()
+    assert all(g is not None for g in runner.graphs)
+    assert all(m.graphs == [None, None] for m in members)   # no per-member graphs
+    for (c, d), m in zip(specs, members):
+        got = m.result()["ez"]
+        assert m.done == 30 and got.shape == (30,)
+        assert rel(got, solo(c, d)) < 1e-9
+
+
 def test_batched_members_equal_solo_runs():
     specs = [(cfg(1.6, 30), GaussianDriver(0.3, 0.8)),
              (cfg(3.25, 25), GaussianDriver(0.05, 1.5)),
