@@ -746,10 +746,14 @@ def main():
 
 
 # DRAM bytes (read + written) per call of each op, summed over all of the
-# op's kernels, from one ncu capture of the small case of the same workload
-# (N=513, window 0.2: 11 xi steps; profiles/launches_production_n513.md).
-NCU_TRAFFIC = {("compute_fields", "fp64"): None, ("compute_fields", "mixed"): None,
-               ("move_deposit", "fp64"): None, ("move_deposit", "mixed"): None}
+# op's kernels, from one ncu capture (dram__bytes_read.sum +
+# dram__bytes_write.sum, cold caches) of the small case of the same workload
+# (N=513, window 0.2: 11 xi steps; profiles/launches_production_n513.md):
+# compute_fields = RHS + four folds + four waves + finish; move_deposit = the
+# fused stage averaged over the xi step's three stages (+ the fixed-point
+# finish in mixed precision).
+NCU_TRAFFIC = {("compute_fields", "fp64"): 197.8e6, ("compute_fields", "mixed"): 128.2e6,
+               ("move_deposit", "fp64"): 110.7e6, ("move_deposit", "mixed"): 124.7e6}
 
 # algorithmic bytes per plasma particle and xi step: K1 64 B (read m, px, py,
 # pz, x_offt, y_offt; write x_offt, y_offt) + 3 x K2 128 B (read 11 x 8 B,
