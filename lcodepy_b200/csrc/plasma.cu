@@ -424,6 +424,18 @@ __device__ __forceinline__ void weights4f(float x, float w[5])
 __device__ __forceinline__ void weights_of(float x, float w[5]) { weights4f(x, w); }
 __device__ __forceinline__ void weights_of(double x, double w[5]) { weights4(x, w); }
 
+// The five weights of a particle whose cell is s (0 or 1) cells past the
+// origin of a six-point footprint, as six weights (zero outside).
+template <typename W>
+__device__ __forceinline__ void shift6(const W w[5], int s, W o[6])
+{
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        const W keep = k < 5 ? w[k] : W(0), moved = k > 0 ? w[k - 1] : W(0);
+        o[k] = s ? moved : keep;
+    }
+}
+
 // Packed FP32 pairs (sm_100 f32x2 arithmetic): two floats in one 64-bit
 // register pair, and an FMA on both lanes.
 __device__ __forceinline__ unsigned long long f32x2(float lo, float hi)
@@ -831,12 +843,82 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
     }
 
     // ---- phase 2: gather ----
+    // Three forms, chosen per warp so that a warp runs one of them: when
+    // every lane's two particles share a cell (or the lane has none), the
+    // 5 x 5 joint form; otherwise lanes whose particles sit in neighbouring
+    // cells gather both over one 6 x 6 footprint (each particle's weights
+    // zero outside its own 5 x 5), and the rest one particle at a time.  The
+    // zero-weight terms leave each particle's sums unchanged.
     FT F0[6] = {0, 0, 0, 0, 0, 0}, F1[6] = {0, 0, 0, 0, 0, 0};
     {
         const int lx = ix[0] - 2 - wx0, ly = iy[0] - 2 - wy0;
         const bool joint = ix[0] >= 0 && ix[0] == ix[1] && iy[0] == iy[1] &&
                            lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY;
-        if (joint && MIXED) {
+        const int mx = min(ix[0], ix[1]), my = min(iy[0], iy[1]);
+        const int px0 = mx - 2 - wx0, py0 = my - 2 - wy0;
+        const bool pair = ix[0] >= 0 && ix[1] >= 0 && abs(ix[1] - ix[0]) <= 1 &&
+                          abs(iy[1] - iy[0]) <= 1 && px0 >= 0 && px0 + 6 <= WX &&
+                          py0 >= 0 && py0 + 6 <= WY;
+        const bool idle = ix[0] < 0 && ix[1] < 0;
+        if (!__all_sync(0xffffffffu, joint || idle)) {
+            if (pair && MIXED) {
+                float ax[6], ay[6], bx[6], by[6], t[5];
+                weights4f((float)xlf[0], t); shift6(t, ix[0] - mx, ax);
+                weights4f((float)ylf[0], t); shift6(t, iy[0] - my, ay);
+                weights4f((float)xlf[1], t); shift6(t, ix[1] - mx, bx);
+                weights4f((float)ylf[1], t); shift6(t, iy[1] - my, by);
+                unsigned long long A[3] = {0ull, 0ull, 0ull}, B[3] = {0ull, 0ull, 0ull};
+#pragma unroll
+                for (int a = 0; a < 6; a++) {
+#pragma unroll
+                    for (int b = 0; b < 6; b++) {
+                        const float wa = ax[a] * ay[b], wb = bx[a] * by[b];
+                        const unsigned long long wa2 = f32x2(wa, wa), wb2 = f32x2(wb, wb);
+                        const int c = (px0 + a) * WY + py0 + b;
+                        const float4 p = reinterpret_cast<const float4 *>(sf)[c];
+                        const float2 q = reinterpret_cast<const float2 *>(sf + 16 * WSZ)[c];
+                        const unsigned long long v3[3] = {f32x2(p.x, p.y), f32x2(p.z, p.w),
+                                                          f32x2(q.x, q.y)};
+#pragma unroll
+                        for (int k = 0; k < 3; k++) {
+                            A[k] = fma_f32x2(v3[k], wa2, A[k]);
+                            B[k] = fma_f32x2(v3[k], wb2, B[k]);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    float lo, hi;
+                    unpack_f32x2(A[k], lo, hi); F0[2 * k] = (FT)lo; F0[2 * k + 1] = (FT)hi;
+                    unpack_f32x2(B[k], lo, hi); F1[2 * k] = (FT)lo; F1[2 * k + 1] = (FT)hi;
+                }
+            } else if (pair) {
+                FT ax[6], ay[6], bx[6], by[6], t[5];
+                weights_of(xlf[0], t); shift6(t, ix[0] - mx, ax);
+                weights_of(ylf[0], t); shift6(t, iy[0] - my, ay);
+                weights_of(xlf[1], t); shift6(t, ix[1] - mx, bx);
+                weights_of(ylf[1], t); shift6(t, iy[1] - my, by);
+#pragma unroll
+                for (int a = 0; a < 6; a++) {
+#pragma unroll
+                    for (int b = 0; b < 6; b++) {
+                        const FT wa = ax[a] * ay[b], wb = bx[a] * by[b];
+                        FT v[6];
+                        FieldWin<FT>::get(sf, WSZ, (px0 + a) * WY + py0 + b, v);
+#pragma unroll
+                        for (int f = 0; f < 6; f++) {
+                            F0[f] += v[f] * wa;
+                            F1[f] += v[f] * wb;
+                        }
+                    }
+                }
+            } else {
+                if (ix[0] >= 0)
+                    gather_one<FT, WX, WY>(sf, fld, N, wx0, wy0, ix[0], iy[0], xlf[0], ylf[0], F0);
+                if (ix[1] >= 0)
+                    gather_one<FT, WX, WY>(sf, fld, N, wx0, wy0, ix[1], iy[1], xlf[1], ylf[1], F1);
+            }
+        } else if (joint && MIXED) {
             // FP32: the window's float4 / float2 of a cell are register pairs
             // (Ex Ey)(Ez Bx)(By Bz), accumulated with packed f32x2 FMAs
             // (per lane the same rounding as the scalar FMAs)
@@ -885,11 +967,6 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
                     }
                 }
             }
-        } else {
-            if (ix[0] >= 0)
-                gather_one<FT, WX, WY>(sf, fld, N, wx0, wy0, ix[0], iy[0], xlf[0], ylf[0], F0);
-            if (ix[1] >= 0)
-                gather_one<FT, WX, WY>(sf, fld, N, wx0, wy0, ix[1], iy[1], xlf[1], ylf[1], F1);
         }
     }
 
@@ -977,13 +1054,47 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
     }
 
     // ---- phase 4: deposit ----
+    // The gather's three forms again (warp-uniform choice), on the new cells.
+    const int mcx = min(cx[0], cx[1]), mcy = min(cy[0], cy[1]);
+    const int dx0 = mcx - 2 - wx0, dy0 = mcy - 2 - wy0;
+    const bool dpair = cx[0] >= 0 && cx[1] >= 0 && abs(cx[1] - cx[0]) <= 1 &&
+                       abs(cy[1] - cy[0]) <= 1 && dx0 >= 0 && dx0 + 6 <= WX && dy0 >= 0 &&
+                       dy0 + 6 <= WY;
+    const bool didle = cx[0] < 0 && cx[1] < 0;
     if constexpr (MIXED) {
         {
             const int lx = cx[0] - 2 - wx0, ly = cy[0] - 2 - wy0;
+            const bool ok = shared_fix_ok(sv[0]) && shared_fix_ok(sv[1]);
             const bool joint = cx[0] >= 0 && cx[0] == cx[1] && cy[0] == cy[1] &&
-                               lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY &&
-                               shared_fix_ok(sv[0]) && shared_fix_ok(sv[1]);
-            if (joint) {
+                               lx >= 0 && lx + 5 <= WX && ly >= 0 && ly + 5 <= WY && ok;
+            if (!__all_sync(0xffffffffu, joint || didle)) {
+                if (dpair && ok) {
+                    double ax[6], ay[6], bx[6], by[6], t[5];
+                    weights4(dxl[0], t); shift6(t, cx[0] - mcx, ax);
+                    weights4(dyl[0], t); shift6(t, cy[0] - mcy, ay);
+                    weights4(dxl[1], t); shift6(t, cx[1] - mcx, bx);
+                    weights4(dyl[1], t); shift6(t, cy[1] - mcy, by);
+#pragma unroll
+                    for (int a = 0; a < 6; a++) {
+#pragma unroll
+                        for (int b = 0; b < 6; b++) {
+                            const double wa = ax[a] * ay[b], wb = bx[a] * by[b];
+                            const int c = (dx0 + a) * WY + dy0 + b;
+#pragma unroll
+                            for (int q = 0; q < 4; q++)
+                                shared_fix_add(swl, swh, q * WSZ + c,
+                                               fma(sv[0][q], wa, fma(sv[1][q], wb, FIX_MAGIC)));
+                        }
+                    }
+                } else {
+                    if (cx[0] >= 0)
+                        deposit_fix_one<WX, WY>(swl, swh, g4, N, wx0, wy0, cx[0], cy[0], dxl[0],
+                                                dyl[0], sv[0]);
+                    if (cx[1] >= 0)
+                        deposit_fix_one<WX, WY>(swl, swh, g4, N, wx0, wy0, cx[1], cy[1], dxl[1],
+                                                dyl[1], sv[1]);
+                }
+            } else if (joint) {
                 double ax[5], ay[5], bx[5], by[5];
                 weights4(dxl[0], ax); weights4(dyl[0], ay);
                 weights4(dxl[1], bx); weights4(dyl[1], by);
@@ -999,11 +1110,6 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
                                            fma(sv[0][q], wa, fma(sv[1][q], wb, FIX_MAGIC)));
                     }
                 }
-            } else {
-                if (cx[0] >= 0)
-                    deposit_fix_one<WX, WY>(swl, swh, g4, N, wx0, wy0, cx[0], cy[0], dxl[0], dyl[0], sv[0]);
-                if (cx[1] >= 0)
-                    deposit_fix_one<WX, WY>(swl, swh, g4, N, wx0, wy0, cx[1], cy[1], dxl[1], dyl[1], sv[1]);
             }
         }
     } else {
@@ -1013,7 +1119,36 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
         double mj = 0;
 #pragma unroll
         for (int q = 0; q < 4; q++) mj = fmax(mj, fabs(sv[0][q]) + fabs(sv[1][q]));
-        if (joint && mj * (0.36 * ih * ih) < FIX56_LIMIT) {
+        const bool ok = mj * (0.36 * ih * ih) < FIX56_LIMIT;
+        if (!__all_sync(0xffffffffu, (joint && ok) || didle)) {
+            if (dpair && ok) {
+                double ax[6], ay[6], bx[6], by[6], t[5];
+                weights4(dxl[0], t); shift6(t, cx[0] - mcx, ax);
+                weights4(dyl[0], t); shift6(t, cy[0] - mcy, ay);
+                weights4(dxl[1], t); shift6(t, cx[1] - mcx, bx);
+                weights4(dyl[1], t); shift6(t, cy[1] - mcy, by);
+#pragma unroll
+                for (int b = 0; b < 6; b++) { ay[b] *= ih; by[b] *= ih; }
+#pragma unroll
+                for (int a = 0; a < 6; a++) {
+                    const double xa = ax[a] * ih, xb = bx[a] * ih;
+#pragma unroll
+                    for (int b = 0; b < 6; b++) {
+                        const double wa = xa * ay[b], wb = xb * by[b];
+                        const int c = (dx0 + a) * WY + dy0 + b;
+#pragma unroll
+                        for (int q = 0; q < 4; q++)
+                            fix56_add(swl, sw1, sw2, q * WSZ + c, fma(sv[0][q], wa, sv[1][q] * wb));
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int p = 0; p < 2; p++)
+                    if (cx[p] >= 0)
+                        deposit_fix56_one<WX, WY>(swl, sw1, sw2, g4, N, ih, wx0, wy0, cx[p], cy[p],
+                                                  dxl[p], dyl[p], sv[p]);
+            }
+        } else if (joint && ok) {
             // the two contributions summed before the fixed-point atomics
             double ax[5], ay[5], bx[5], by[5];
             weights4(dxl[0], ax); weights4(dyl[0], ay);
@@ -1032,12 +1167,6 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
                         fix56_add(swl, sw1, sw2, q * WSZ + c, fma(sv[0][q], wa, sv[1][q] * wb));
                 }
             }
-        } else {
-#pragma unroll
-            for (int p = 0; p < 2; p++)
-                if (cx[p] >= 0)
-                    deposit_fix56_one<WX, WY>(swl, sw1, sw2, g4, N, ih, wx0, wy0, cx[p], cy[p],
-                                              dxl[p], dyl[p], sv[p]);
         }
     }
     __syncthreads();
