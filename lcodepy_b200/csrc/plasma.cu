@@ -606,13 +606,16 @@ __device__ __forceinline__ void deposit_fix_one(unsigned *swl, int *swh, fix_t *
 // particle of the block at most once), no word overflows.  The integer sums
 // are exact and independent of the order of the atomics; each contribution
 // differs from FP64 by at most 2^-57, and the flush recombines the words
-// with one FP64 rounding before adding the value to the outputs.
+// with one FP64 rounding before adding the value to the outputs.  The
+// particle's values arrive multiplied by 2^56 (exact: a power of two), so a
+// contribution's integer is one rounding conversion of its product.
 constexpr double FIX56_SCALE = 72057594037927936.0;   // 2^56
-constexpr double FIX56_LIMIT = 16.0;                  // per contribution, in the window
+constexpr double FIX56_LIMIT = 16.0 * FIX56_SCALE;    // per contribution, in the window
 
+// v: a contribution in units of 2^-56
 __device__ __forceinline__ void fix56_add(unsigned *w0, unsigned *w1, int *w2, int idx, double v)
 {
-    const long long c = __double2ll_rn(v * FIX56_SCALE);
+    const long long c = __double2ll_rn(v);
     atomicAdd(w0 + idx, (unsigned)c & 0xFFFFFu);
     atomicAdd(w1 + idx, (unsigned)(c >> 20) & 0xFFFFFu);
     atomicAdd(w2 + idx, (int)(c >> 40));
@@ -625,7 +628,8 @@ __device__ __forceinline__ double fix56_value(unsigned w0, unsigned w1, int w2)
 
 // One particle's FP64 deposit (weights.py:151-190 arithmetic, w = (wx / h)
 // (wy / h)) into the three-word window, or into HBM with FP64 atomics when
-// the stencil leaves the window or a contribution could leave the range.
+// the stencil leaves the window or a contribution could leave the range;
+// sv: the particle's values in units of 2^-56.
 template <int WX, int WY>
 __device__ __forceinline__ void deposit_fix56_one(unsigned *w0, unsigned *w1, int *w2, double *const *g,
                                                   int N, double ih, int wx0, int wy0, int cx, int cy,
@@ -654,7 +658,7 @@ __device__ __forceinline__ void deposit_fix56_one(unsigned *w0, unsigned *w1, in
             } else {
                 const int64_t c = (int64_t)(cx + a - 2) * N + cy + b - 2;
 #pragma unroll
-                for (int q = 0; q < 4; q++) atomicAdd(g[q] + c, sv[q] * w);
+                for (int q = 0; q < 4; q++) atomicAdd(g[q] + c, sv[q] * w * (1.0 / FIX56_SCALE));
             }
         }
     }
@@ -1047,9 +1051,9 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
             continue;
         }
         cx[p] = c_x; cy[p] = c_y;
-        // mixed: values scaled to fixed-point units (with the 1/h^2 of the
-        // weights); FP64: the values themselves
-        const double sc = MIXED ? FIX_SCALE * ih * ih : 1.0;
+        // values in fixed-point units: mixed, 2^32 (with the 1/h^2 of the
+        // weights); FP64, 2^56
+        const double sc = MIXED ? FIX_SCALE * ih * ih : FIX56_SCALE;
         sv[p][0] = dro * sc; sv[p][1] = djx * sc; sv[p][2] = djy * sc; sv[p][3] = djz * sc;
     }
 
