@@ -356,9 +356,10 @@ def run_batch(args, ws, rank, local):
 def run_plain_requests(reqs, dev, extra=None):
     """Run each (arrival, id, config, driver) request alone through the
     drop-in Simulation API in FP64 (config keys in `extra` added); returns
-    {id: {seconds, ez}}.  A beam driver's particle file is written before its
-    clock starts (the served path generates beams on the device in
-    milliseconds)."""
+    {id: {seconds, ez}}, or {id: {seconds, error}} for a request whose run
+    raised (a device error word: a runaway plasma particle).  A beam
+    driver's particle file is written before its clock starts (the served
+    path generates beams on the device in milliseconds)."""
     import torch
     from lcodepy_b200 import Simulation
     from lcodepy_b200.batch import BeamDriver
@@ -376,17 +377,22 @@ def run_plain_requests(reqs, dev, extra=None):
                 del beam
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            with contextlib.redirect_stdout(sys.stderr):   # Simulation's progress notes
-                if path is None:
-                    sim = Simulation(config=c, beam_parameters=drv, runas_filename='')
-                    sim.step()
-                else:
-                    sim = Simulation(config=c, runas_filename='')
-                    sim.load_beamfile(path)
-                    sim.step(1)
-            ez = sim.push_solver.ez_axis.cpu().numpy()
-            torch.cuda.synchronize()
-            out[rid] = {"seconds": time.perf_counter() - t0, "ez": ez}
+            sim = None
+            try:
+                with contextlib.redirect_stdout(sys.stderr):   # Simulation's progress notes
+                    if path is None:
+                        sim = Simulation(config=c, beam_parameters=drv, runas_filename='')
+                        sim.step()
+                    else:
+                        sim = Simulation(config=c, runas_filename='')
+                        sim.load_beamfile(path)
+                        sim.step(1)
+                ez = sim.push_solver.ez_axis.cpu().numpy()
+                torch.cuda.synchronize()
+                out[rid] = {"seconds": time.perf_counter() - t0, "ez": ez}
+            except RuntimeError as e:
+                torch.cuda.synchronize()
+                out[rid] = {"seconds": time.perf_counter() - t0, "error": str(e)}
             del sim
     return out
 
@@ -458,7 +464,8 @@ def run_serve(args, ws, rank, local):
     # accuracy: every served result against the same request alone in FP64
     def rel_l2(a, b):
         return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
-    err_of = {rid: rel_l2(done[rid]["ez"], plain[rid]["ez"]) for rid in plain}
+    plain_failed = sorted(rid for rid, v in plain.items() if "error" in v)
+    err_of = {rid: rel_l2(done[rid]["ez"], v["ez"]) for rid, v in plain.items() if "ez" in v}
     errs = list(err_of.values())
     worst = sorted(err_of.items(), key=lambda kv: -kv[1])[:3]
     # requests over 1e-5 run once more in FP64 with the reference's three
@@ -467,7 +474,9 @@ def run_serve(args, ws, rank, local):
     over = [r for r in reqs if r[1] in err_of and err_of[r[1]] > 1e-5]
     alt = run_plain_requests(over, dev, extra={'fused-particle-kernels': False})
     fp64_spread = {rid: {"mixed_vs_fp64": err_of[rid],
-                         "fp64_vs_fp64_separate_kernels": rel_l2(alt[rid]["ez"], plain[rid]["ez"])}
+                         "fp64_vs_fp64_separate_kernels": (
+                             rel_l2(alt[rid]["ez"], plain[rid]["ez"]) if "ez" in alt[rid]
+                             else alt[rid]["error"])}
                    for rid in alt}
     return {"value": value, "ms": ms, "wall_s": wall, "cell_steps": cell_steps,
             "p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
@@ -476,6 +485,7 @@ def run_serve(args, ws, rank, local):
             "plain_busy_s": sum(v["seconds"] for v in plain.values()), "failed": failed,
             "beam_requests": sum(isinstance(r[3], BeamDriver) for r in reqs),
             "errs": errs, "worst": worst, "fp64_spread": fp64_spread,
+            "plain_failed": plain_failed,
             "clocks": clocks, "launches": launches,
             "span_arrivals_s": reqs[-1][0]}
 
@@ -556,7 +566,8 @@ def run_headline(args, ws, rank, local):
                                   "over_1e-5": int(sum(e > 1e-5 for e in v["errs"])),
                                   "worst": v["worst"],
                                   "over_1e-5_fp64_spread": v["fp64_spread"]},
-            "failed_requests": v["failed"], "gpu_launches": v["launches"],
+            "failed_requests": v["failed"],
+            "plain_fp64_failed_requests": v["plain_failed"], "gpu_launches": v["launches"],
             "clocks": v["clocks"]}
     except Exception as e:
         out["served"] = {"error": f"{type(e).__name__}: {e}"}
@@ -690,6 +701,7 @@ def main():
                            "l2": "aggregate member state larger than L2"},
                 "latency_s": {"p50": r["p50"], "p99": r["p99"]},
                 "failed_requests": r["failed"],
+                "plain_fp64_failed_requests": r["plain_failed"],
                 "makespan_s": r["ms"] / 1e3, "cell_steps": r["cell_steps"],
                 "plain_fp64": {"value": r["plain_value"], "p50": r["plain_p50"],
                                "p99": r["plain_p99"], "busy_s": r["plain_busy_s"]},
@@ -766,8 +778,8 @@ def main():
 # compute_fields = RHS + four folds + four waves + finish; move_deposit = the
 # fused stage averaged over the xi step's three stages (+ the fixed-point
 # finish in mixed precision).
-NCU_TRAFFIC = {("compute_fields", "fp64"): 197.8e6, ("compute_fields", "mixed"): 128.2e6,
-               ("move_deposit", "fp64"): 110.7e6, ("move_deposit", "mixed"): 124.7e6}
+NCU_TRAFFIC = {("compute_fields", "fp64"): 197.9e6, ("compute_fields", "mixed"): 128.2e6,
+               ("move_deposit", "fp64"): 111.4e6, ("move_deposit", "mixed"): 125.4e6}
 
 # algorithmic bytes per plasma particle and xi step: K1 64 B (read m, px, py,
 # pz, x_offt, y_offt; write x_offt, y_offt) + 3 x K2 128 B (read 11 x 8 B,

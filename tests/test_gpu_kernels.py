@@ -175,6 +175,68 @@ def test_deposit_runaway_particles_take_global_path(kat):
         close(N_(o[0]), getattr(cur, k)[0], 1e-12, "K3 " + k)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_fused_stage_forms_match_separate_kernels(precision):
+    """The fused first stage (K1 + K2 + K3 in one kernel) against the three
+    kernels run separately, on a lattice whose particles are scattered so
+    that every form of the fused gather and deposit runs: both particles of
+    a thread in one cell, in neighbouring cells (the shared 6 x 6
+    footprint), further apart, and outside the block's window (global
+    atomics).  FP64 to 1e-12; mixed precision (FP32 gather, fixed-point
+    deposit) to 1e-5 of the FP64 kernels, and bit-identical over two calls."""
+    from lcodepy_b200.config import Config
+    from lcodepy_b200.solver import CurrentSet, Plane2d3vPlasmaSolver
+    cfg = Config({'geometry': '3d', 'window-width': 12.85, 'transverse-step': 0.1,
+                  'xi-step': 0.1, 'window-length': 1.0, 'ion-model': 'background',
+                  'plasma-particles-per-cell': 4, 'precision': precision, 'print-every': 0})
+    cfg._adjust_config_values_3d()
+    ps = Plane2d3vPlasmaSolver(cfg, DEV)
+    ps.init_state(0.0)
+    prev, full = ps.states
+    N, h, n = ps.N, ps.h, prev.n_per_sort
+    rng = np.random.default_rng(11)
+    xi, yi = N_(prev.x_init), N_(prev.y_init)
+    inner = (np.abs(xi) < ps.boundary - 12 * h) & (np.abs(yi) < ps.boundary - 12 * h)
+    u = rng.random(n)
+    mag = np.where(u < 0.4, 0.2, np.where(u < 0.9, 1.2, np.where(inner, 7.0, 1.2))) * h
+    prev.x_offt.copy_(T(rng.uniform(-1, 1, n) * mag))
+    prev.y_offt.copy_(T(rng.uniform(-1, 1, n) * mag))
+    m = N_(prev.m)
+    for k in ("px", "py", "pz"):    # |p| / m ~ 0.3: velocities up to ~0.7 c
+        getattr(prev, k).copy_(T(rng.normal(0.0, 0.3, n) * m))
+    F = ps.fields[0]
+    F.buf.copy_(T(rng.uniform(-0.05, 0.05, (7, N, N))))
+
+    def particles():
+        return {k: N_(getattr(full, k)).copy() for k in ("x_offt", "y_offt", "px", "py", "pz", "q")}
+
+    # the reference's three kernels, FP64 push, deposit in the stage's precision
+    cs = CurrentSet(N, DEV)
+    ps._move_wo_fields(prev, full)
+    ps._move_smart(F, prev, full)
+    ps._deposit(full, cs)
+    torch.cuda.synchronize()
+    sep_p, sep_c = particles(), N_(cs.buf).copy()
+    assert int(ps.err.item()) == 0
+    runs = []
+    for _ in range(2):
+        cf = CurrentSet(N, DEV)
+        ps._move_deposit(F, prev, full, cf, True)
+        torch.cuda.synchronize()
+        runs.append((particles(), N_(cf.buf).copy()))
+    assert int(ps.err.item()) == 0
+    rel = 1e-12 if precision == "fp64" else 1e-5
+    fus_p, fus_c = runs[0]
+    for k in sep_p:
+        close(fus_p[k], sep_p[k], rel, "fused " + k)
+    for i, k in enumerate(("ro", "jx", "jy", "jz")):
+        close(fus_c[i], sep_c[i], rel, "fused " + k)
+    if precision == "mixed":
+        for k in fus_p:
+            np.testing.assert_array_equal(runs[1][0][k], fus_p[k])
+        np.testing.assert_array_equal(runs[1][1], fus_c)
+
+
 def _fields_args(d, precision, ops, outs, ws):
     N = int(d["N"])
     keep = []
