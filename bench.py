@@ -443,6 +443,7 @@ def run_serve(args, ws, rank, local):
     ms = max_over_ranks(t0.elapsed_time(t1), ws)
     done = {r: d for r, d in srv.done.items() if "error" not in d}
     failed = len(srv.done) - len(done)
+    failed_ids = {r: d["error"][:160] for r, d in sorted(srv.done.items()) if "error" in d}
     cell_steps = sum(d["cells"] * d["steps"] for d in done.values())
     lat = np.array([done[r]["latency"] for _, r, _, _ in reqs if r in done])
     value = ws * cell_steps / (ms / 1e3)
@@ -485,7 +486,7 @@ def run_serve(args, ws, rank, local):
             "plain_busy_s": sum(v["seconds"] for v in plain.values()), "failed": failed,
             "beam_requests": sum(isinstance(r[3], BeamDriver) for r in reqs),
             "errs": errs, "worst": worst, "fp64_spread": fp64_spread,
-            "plain_failed": plain_failed,
+            "plain_failed": plain_failed, "failed_ids": failed_ids,
             "clocks": clocks, "launches": launches,
             "span_arrivals_s": reqs[-1][0]}
 
@@ -566,7 +567,7 @@ def run_headline(args, ws, rank, local):
                                   "over_1e-5": int(sum(e > 1e-5 for e in v["errs"])),
                                   "worst": v["worst"],
                                   "over_1e-5_fp64_spread": v["fp64_spread"]},
-            "failed_requests": v["failed"],
+            "failed_requests": v["failed"], "failed_ids": v["failed_ids"],
             "plain_fp64_failed_requests": v["plain_failed"], "gpu_launches": v["launches"],
             "clocks": v["clocks"]}
     except Exception as e:
@@ -700,7 +701,7 @@ def main():
                            "steps_are": "requests; ms_per_step = makespan / requests",
                            "l2": "aggregate member state larger than L2"},
                 "latency_s": {"p50": r["p50"], "p99": r["p99"]},
-                "failed_requests": r["failed"],
+                "failed_requests": r["failed"], "failed_ids": r["failed_ids"],
                 "plain_fp64_failed_requests": r["plain_failed"],
                 "makespan_s": r["ms"] / 1e3, "cell_steps": r["cell_steps"],
                 "plain_fp64": {"value": r["plain_value"], "p50": r["plain_p50"],
