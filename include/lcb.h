@@ -285,17 +285,20 @@ typedef struct lcb_beam_step_args {
     lcb_beam_soa stage;                /* scratch, >= fresh + fell particles */
     uint8_t *stage_flags;
     int64_t stage_capacity;
-    double *ro0, *ro1;                 /* beam density: this step's and the next */
+    double *ro0, *ro1;                 /* beam density: this step's and the next
+                                          (ro1 is cleared first: N*N doubles) */
     const lcb_fields *fields_k, *fields_k1;  /* previous and new plasma fields */
     int *err;
 } lcb_beam_step_args;
 
-/* One xi step of the beam with every count kept on the device: deposit the
- * layout layer, push layer i-1 (fresh particles get their substep sizes
- * first) followed by the particles that fell from the previous push, then
- * compact in order: moved -> drain, fell -> fell_out, lost -> lost.  The
- * deposit only reads the source, so a caller may lay out layer i+1 right
- * after the plasma step of layer i.  Replaces the per-layer
+/* One xi step of the beam with every count kept on the device: push layer
+ * i-1 (fresh particles get their substep sizes first) followed by the
+ * particles that fell from the previous push, compact in order: moved ->
+ * drain, fell -> fell_out, lost -> lost; then deposit the layout layer into
+ * ro0 and ro1, ro1 having been cleared by the push's grid (with three
+ * rotating planes it last held the density that the plasma step of layer i
+ * has just read).  The deposit only reads the source, so a caller may lay
+ * out layer i+1 right after the plasma step of layer i.  Replaces the per-layer
  * body of PusherAndSolver3D.step_dt for a non-rigid beam,
  * lcode/push_solvers/push_solver.py:237-261 (layout_beam_layer,
  * move_beam_layer, create_next_layer, push_beam_layer). */

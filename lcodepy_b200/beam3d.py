@@ -323,7 +323,7 @@ class BeamCalculator:
         between fields_prev and fields_new, then lay out layer i+1.  The
         argument struct is built once per fell-buffer parity; a step only
         sets its layer indices, ranges, planes and fields."""
-        self.planes[(i + 2) % 3].zero_()
+        # plane (i + 2) % 3 (ro1) is cleared inside lcb_beam_step
         a = self._step_args_cache.get(self.fell_cur)
         if a is None:
             a = self._step_args_cache[self.fell_cur] = self._args(i, (0, 0), (0, 0), None, None)
@@ -355,7 +355,9 @@ class RigidBeamCalculator:
     """Rigid driver (beam_calculator.py:148-181): rho_b(xi) = fn(xp, xi, X, Y)
     with X, Y = meshgrid(grid, grid).  The function is evaluated on the host
     with numpy, for all xi layers of a time step at once, and the planes are
-    uploaded to HBM in one copy."""
+    uploaded to HBM in one copy.  Each xi step copies its layer into one of
+    two fixed planes (the other holds the previous layer), so the plasma
+    step's captured graphs read fixed addresses: one device copy per step."""
 
     def __init__(self, config: Config, device=None):
         self.device = device or torch.device("cuda", torch.cuda.current_device())
@@ -368,6 +370,7 @@ class RigidBeamCalculator:
         self.rho_divisor = 1.0
         self.table = None
         self.zero = torch.zeros(N, N, dtype=torch.float64, device=self.device)
+        self.planes = torch.zeros(2, N, N, dtype=torch.float64, device=self.device)
 
     def start_time_step(self):
         pass
@@ -385,8 +388,9 @@ class RigidBeamCalculator:
         self._host = host
 
     def layout_beam_layer(self, fn, layer_idx):
-        full = self.table[layer_idx - self.first]
-        prev = self.table[layer_idx - 1 - self.first] if layer_idx > self.first else self.zero
+        full = self.planes[layer_idx % 2]
+        full.copy_(self.table[layer_idx - self.first])
+        prev = self.planes[(layer_idx - 1) % 2] if layer_idx > self.first else self.zero
         return full, prev
 
     def move_beam_layer(self, *a, **k):

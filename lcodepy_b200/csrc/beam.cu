@@ -197,6 +197,8 @@ struct StepArgs {
     double e_sub, time_step;
     PushParams P;
     FieldPair F;
+    double *clear;          // plane zeroed by the same grid (the next layout's lower plane)
+    int64_t clear_n;
     int *err;
 };
 
@@ -220,6 +222,9 @@ __device__ __forceinline__ void soa_store(const lcb_beam_soa &s, int64_t i, cons
 
 __global__ void __launch_bounds__(128) k_beam_push_stage(StepArgs a)
 {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < a.clear_n;
+         t += (int64_t)gridDim.x * blockDim.x)
+        a.clear[t] = 0.0;
     const int64_t total = a.n_fresh + *a.fell_in_count;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
          t += (int64_t)gridDim.x * blockDim.x) {
@@ -420,17 +425,9 @@ extern "C" int lcb_beam_step(const lcb_beam_step_args *a, void *stream)
     LCB_REQUIRE(a->move_end - a->move_begin <= a->stage_capacity,
                 "stage capacity %lld < fresh layer %lld", (long long)a->stage_capacity,
                 (long long)(a->move_end - a->move_begin));
+    LCB_REQUIRE(a->ro0 && a->ro1, "density planes are NULL");
     cudaStream_t st = as_stream(stream);
     const int N = a->grid_steps;
-    if (a->layout_end > a->layout_begin) {
-        LCB_REQUIRE(a->ro0 && a->ro1, "density planes are NULL");
-        const int64_t n = a->layout_end - a->layout_begin, o = a->layout_begin;
-        k_beam_deposit<<<grid_for(n, 128), 128, 0, st>>>(
-            n, N, a->h, a->xi_step, -a->xi_step * (double)a->layout_idx,
-            a->source.x + o, a->source.y + o, a->source.xi + o, a->source.q_norm + o,
-            a->ro0, a->ro1, a->err);
-        LCB_LAUNCH_CHECK("k_beam_deposit");
-    }
     StepArgs s;
     s.src = a->source; s.fin = a->fell_in; s.stage = a->stage;
     s.move_begin = a->move_begin; s.n_fresh = a->move_end - a->move_begin;
@@ -446,6 +443,8 @@ extern "C" int lcb_beam_step(const lcb_beam_step_args *a, void *stream)
         s.F.k1[c] = a->fields_k1->f[c];
         LCB_REQUIRE(s.F.k[c] && s.F.k1[c], "field plane %d is NULL", c);
     }
+    s.clear = a->ro1;
+    s.clear_n = (int64_t)N * N;
     s.err = a->err;
     k_beam_push_stage<<<2 * sm_count(), 128, 0, st>>>(s);
     LCB_LAUNCH_CHECK("k_beam_push_stage");
@@ -461,5 +460,14 @@ extern "C" int lcb_beam_step(const lcb_beam_step_args *a, void *stream)
     c.err = a->err;
     k_beam_compact<<<1, CMP_THREADS, 0, st>>>(c);
     LCB_LAUNCH_CHECK("k_beam_compact");
+    // the layout reads only the source and ro1 was cleared by the push grid
+    if (a->layout_end > a->layout_begin) {
+        const int64_t n = a->layout_end - a->layout_begin, o = a->layout_begin;
+        k_beam_deposit<<<grid_for(n, 128), 128, 0, st>>>(
+            n, N, a->h, a->xi_step, -a->xi_step * (double)a->layout_idx,
+            a->source.x + o, a->source.y + o, a->source.xi + o, a->source.q_norm + o,
+            a->ro0, a->ro1, a->err);
+        LCB_LAUNCH_CHECK("k_beam_deposit");
+    }
     return LCB_OK;
 }

@@ -114,6 +114,22 @@ class Plane2d3vPlasmaSolver:
         # synchronisation of torch.cuda.graph, for solvers that share the GPU
         # with others (batch members)
         self.capture_on_stream = False
+        # on-axis Ez of every xi step recorded on the device as the step's
+        # last kernel (inside the captured graphs): a history and its counter
+        # (see record_axis); None records nothing
+        self.axis = None
+
+    def record_axis(self, capacity: int):
+        """Record the new on-axis Ez at the end of every xi step into a
+        device history of ``capacity`` entries (lcb_record_axis); returns
+        (history, counter).  The buffers persist, so captured graphs stay
+        valid; a larger capacity drops the graphs."""
+        if self.axis is None or self.axis[0].numel() < capacity:
+            self.axis = (torch.zeros(capacity, dtype=torch.float64, device=self.device),
+                         torch.zeros(1, dtype=torch.int64, device=self.device))
+            self.graphs = [None, None]
+            self.plane_graphs = {}
+        return self.axis
 
     def _timed(self, name, fn, *args):
         if self.op_timers is None:
@@ -371,6 +387,11 @@ class Plane2d3vPlasmaSolver:
         else:
             T("move_smart", self._move_smart, hB, prev, full)
             T("deposit", self._deposit, full, cf)
+        if self.axis is not None:
+            hist, counter = self.axis
+            _lib.check(_lib.load().lcb_record_axis(
+                Ff.buf[FIELD_NAMES.index("Ez")].data_ptr(), self.N, counter.data_ptr(),
+                hist.data_ptr(), hist.numel(), _lib.stream_handle()), "lcb_record_axis")
         if advance:
             self.cur = f
             self.last_fields = Fp
