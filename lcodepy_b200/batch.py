@@ -17,12 +17,21 @@ is launched beside it on the member's stream, without host round trips.
 ``Server`` admits requests that arrive over time into free slots while others
 run (continuous batching), bounded by an HBM budget, and reports each
 request's completion latency.
+
+Slots can be checkpointed between xi steps and resumed (``Member.checkpoint``,
+``restore_member``, ``Server.checkpoint`` / ``Server.restore``): a member's
+plasma state goes to a plasma state file in the format the reference's
+``Simulation`` loads with ``external_plasmastate`` (plasma_state.py), its
+metadata (config, driver, steps done, on-axis Ez so far, and for a beam
+driver the beam step's device buffers) to a slot file beside it.
 """
 from __future__ import annotations
 
 import collections
 import dataclasses
+import json
 import math
+import os
 import time
 
 import numpy as np
@@ -169,6 +178,7 @@ class Member:
 
     def __init__(self, config: dict, driver: GaussianDriver, device=None, name=None):
         self.device = device or torch.device("cuda", torch.cuda.current_device())
+        self.config_dict = dict(config)
         cfg = Config({**config, 'cuda-graphs': False})
         cfg._adjust_config_values_3d()
         self.config = cfg
@@ -266,6 +276,37 @@ class Member:
         return {"ez": self.ez.cpu().numpy(),
                 "fields": self.solver.prev_fields.buf.cpu().numpy()}
 
+    def checkpoint(self, directory) -> str:
+        """Write this member's state between xi steps: ``<name>.plasma.npz``
+        (a plasma state file: the last computed layer's particles, fields,
+        currents and background charge, with its xi) and ``<name>.slot.npz``
+        (config, driver, steps done, on-axis Ez so far, driver-specific
+        state).  Waits for the member's stream; raises if a device error word
+        is set.  Returns the common path prefix for ``restore_member``."""
+        from .plasma_state import save_plasmastate
+        self.check()
+        os.makedirs(directory, exist_ok=True)
+        base = os.path.join(directory, str(self.name if self.name is not None else "member"))
+        ps = self.solver
+        save_plasmastate(base + ".plasma.npz", ps.particles_dict(), ps.prev_fields.arrays(),
+                         ps.prev_currents.arrays(), ro_initial=ps.ro_initial,
+                         xi_plasma_layer=-self.dxi * (self.done - 1))
+        meta = {"format": np.array(SLOT_FORMAT), "name": np.array(str(self.name)),
+                "config": np.array(json.dumps(self.config_dict)),
+                "driver": np.array(driver_record(self.driver)),
+                "done": np.array(self.done),
+                "ez": self.ez[:self.done].cpu().numpy(),
+                "arrival": np.array(float(getattr(self, "t_arrival", 0.0) or 0.0))}
+        meta.update(self._slot_state())
+        np.savez(base + ".slot.npz", **meta)
+        return base
+
+    def _slot_state(self) -> dict:
+        return {}
+
+    def _restore_slot_state(self, meta: dict):
+        pass
+
     def release(self):
         self.graphs = [None, None]
         self.solver = None
@@ -282,6 +323,7 @@ class BeamMember(Member):
     def __init__(self, config: dict, driver: BeamDriver, device=None, name=None):
         from .beam3d import BeamCalculator, BeamSource
         self.device = device or torch.device("cuda", torch.cuda.current_device())
+        self.config_dict = dict(config)
         cfg = Config(config)
         cfg._adjust_config_values_3d()
         self.config = cfg
@@ -333,6 +375,35 @@ class BeamMember(Member):
         if e:
             raise RuntimeError(f"beam device error word 0x{e:x} in member {self.name}")
 
+    def _beam_buffers(self):
+        bc = self.bc
+        return (("drain", bc.drain, 2), ("lost", bc.lost, 3), ("fell0", bc.fell[0], 0),
+                ("fell1", bc.fell[1], 1))
+
+    def _slot_state(self) -> dict:
+        """The beam step's state between xi steps: the three density planes
+        (layouts in progress), the device counters, the fell-buffer parity
+        and the filled part of the drain, lost and fell buffers.  The source
+        beam is regenerated from the driver's seed."""
+        bc = self.bc
+        counts = bc.counts.cpu().numpy()
+        out = {"beam_planes": bc.planes.cpu().numpy(), "beam_counts": counts,
+               "beam_fell_cur": np.array(bc.fell_cur)}
+        for tag, buf, c in self._beam_buffers():
+            for k in buf._all():
+                out[f"beam_{tag}_{k}"] = getattr(buf, k)[:int(counts[c])].cpu().numpy()
+        return out
+
+    def _restore_slot_state(self, meta: dict):
+        bc = self.bc
+        bc.planes.copy_(torch.from_numpy(meta["beam_planes"]))
+        bc.counts.copy_(torch.from_numpy(meta["beam_counts"]))
+        bc.fell_cur = int(meta["beam_fell_cur"])
+        for tag, buf, _ in self._beam_buffers():
+            for k in buf._all():
+                a = torch.from_numpy(meta[f"beam_{tag}_{k}"])
+                getattr(buf, k)[:a.numel()].copy_(a)
+
     def release(self):
         self.solver = None
         self.bc = None
@@ -345,6 +416,52 @@ def make_member(config: dict, driver, device=None, name=None) -> Member:
     if isinstance(driver, BeamDriver):
         return BeamMember(config, driver, device, name)
     return Member(config, driver, device, name)
+
+
+SLOT_FORMAT = 1
+
+
+def driver_record(driver) -> str:
+    """A driver as JSON (kind and parameters)."""
+    kind = "beam" if isinstance(driver, BeamDriver) else "rigid"
+    return json.dumps({"kind": kind, **dataclasses.asdict(driver)})
+
+
+def driver_from_record(record: str):
+    d = json.loads(record)
+    kind = d.pop("kind")
+    if kind == "beam":
+        return BeamDriver(**d)
+    if kind == "rigid":
+        return GaussianDriver(**d)
+    raise ValueError(f"unknown driver kind {kind!r}")
+
+
+def restore_member(base: str, device=None) -> Member:
+    """Rebuild a member from ``Member.checkpoint``'s files (``base`` is the
+    path prefix it returned) and put it where it stopped: the next step is
+    the one after the stored layer."""
+    from .plasma_state import load_plasmastate
+    with np.load(base + ".slot.npz") as z:
+        meta = {k: z[k] for k in z.files}
+    if int(meta["format"]) != SLOT_FORMAT:
+        raise ValueError(f"{base}.slot.npz: slot format {int(meta['format'])}, "
+                         f"expected {SLOT_FORMAT}")
+    config = json.loads(str(meta["config"]))
+    driver = driver_from_record(str(meta["driver"]))
+    m = make_member(config, driver, device, name=str(meta["name"]))
+    state = load_plasmastate(base + ".plasma.npz", m.solver.sort_names)
+    done = int(meta["done"])
+    with torch.cuda.stream(m.stream):
+        m.solver.load_state(state)
+        m.counter.fill_(done)
+        if done:
+            m.ez[:done].copy_(torch.from_numpy(meta["ez"]))
+        m._restore_slot_state(meta)
+    m.stream.synchronize()
+    m.done = done
+    m.t_arrival = float(meta["arrival"])
+    return m
 
 
 def solo_ez(config: dict, driver, **overrides) -> np.ndarray:
@@ -648,6 +765,49 @@ class Server:
 
     def idle(self):
         return not self.running and not self.draining and not self.waiting
+
+    def checkpoint(self, directory):
+        """Write the server's requests to ``directory``: requests whose steps
+        are all issued are finished first (their results stay in ``done``),
+        every running request's slot is written (``Member.checkpoint``) and
+        the waiting queue goes to ``server.json`` with the arrival times
+        relative to now.  The server itself is left as it was."""
+        for m in list(self.draining):
+            m.end_event.synchronize()
+        self.retire()
+        os.makedirs(directory, exist_ok=True)
+        t = self.now()
+        running = []
+        for m in self.running:
+            base = m.checkpoint(directory)
+            running.append({"base": os.path.basename(base), "arrival": m.t_arrival - t})
+        waiting = [{"id": rid, "config": cfg, "driver": driver_record(drv),
+                    "arrival": arr - t} for arr, rid, cfg, drv in self.waiting]
+        with open(os.path.join(directory, "server.json"), "w") as f:
+            json.dump({"format": SLOT_FORMAT, "running": running, "waiting": waiting}, f)
+
+    @classmethod
+    def restore(cls, directory, hbm_budget_bytes: int, max_slots: int = 64, device=None):
+        """A server holding ``checkpoint``'s requests: the running ones
+        admitted at once (in their stored state), the waiting ones queued
+        with their arrival times relative to the restore."""
+        srv = cls(hbm_budget_bytes, max_slots, device)
+        with open(os.path.join(directory, "server.json")) as f:
+            meta = json.load(f)
+        if meta.get("format") != SLOT_FORMAT:
+            raise ValueError(f"{directory}/server.json: format {meta.get('format')}, "
+                             f"expected {SLOT_FORMAT}")
+        for r in meta["running"]:
+            m = restore_member(os.path.join(directory, r["base"]), srv.device)
+            m.t_arrival = r["arrival"]
+            m.t_admit = 0.0
+            m.footprint = footprint_bytes(m.config_dict, m.driver)
+            srv.running.append(m)
+            srv.used += m.footprint
+        for w in meta["waiting"]:
+            srv.submit(w["id"], w["config"], driver_from_record(w["driver"]),
+                       arrival=max(0.0, w["arrival"]))
+        return srv
 
     def run(self):
         """Serve until every submitted request is done."""

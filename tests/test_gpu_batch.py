@@ -99,3 +99,59 @@ def test_server_results_same_alone_and_in_the_mix():
     assert any(d[x]["admitted"] >= d[y]["finished"] for x in d for y in d if x != y)
     for rid, (c, d) in specs.items():
         assert rel(srv.done[rid]["ez"], solo_ez(c, d)) < 1e-9, rid
+
+
+def _steps(m, n):
+    for _ in range(n):
+        m.step()
+    m.stream.synchronize()
+
+
+@pytest.mark.parametrize("kind,precision", [("rigid", "fp64"), ("rigid", "mixed"),
+                                            ("beam", "fp64")])
+def test_member_checkpoint_and_resume(tmp_path, kind, precision):
+    """A member written between xi steps (plasma state file + slot file) and
+    rebuilt by restore_member continues to the result of an uninterrupted
+    run; writing the checkpoint leaves the running member unchanged."""
+    from lcodepy_b200.batch import make_member, restore_member
+    n, k = 40, 17
+    c = cfg(1.6, n, precision=precision)
+    d = GaussianDriver(0.3, 0.8) if kind == "rigid" else _beam(5, 0.3)
+    ref = make_member(c, d, name="ref")
+    _steps(ref, n)
+    want = ref.result()
+    m = make_member(c, d, name="slot")
+    _steps(m, k)
+    base = m.checkpoint(str(tmp_path))
+    _steps(m, n - k)
+    r = restore_member(base)
+    assert r.done == k and r.name == "slot" and r.config_dict == c
+    _steps(r, n - k)
+    tol = 1e-12
+    for got in (m.result(), r.result()):
+        assert rel(got["ez"], want["ez"]) < tol
+        assert rel(got["fields"], want["fields"]) < tol
+    assert np.abs(want["ez"]).max() > 0
+
+
+def test_server_checkpoint_and_restore(tmp_path):
+    """A server checkpointed with requests running and waiting, rebuilt by
+    Server.restore: every request finishes with its solo result."""
+    specs = {"r0": (cfg(1.6, 30), GaussianDriver(0.3, 0.8)),
+             "r1": (cfg(1.6, 40), _beam(4, 0.3)),
+             "r2": (cfg(3.25, 25), GaussianDriver(0.1, 1.2))}
+    srv = Server(hbm_budget_bytes=8 << 30, max_slots=2)
+    for rid, (c, d) in specs.items():
+        srv.submit(rid, c, d, arrival=0.0)
+    srv.poll()
+    for _ in range(10):
+        srv.tick()
+    assert [m.name for m in srv.running] == ["r0", "r1"] and len(srv.waiting) == 1
+    srv.checkpoint(str(tmp_path))
+    srv2 = Server.restore(str(tmp_path), hbm_budget_bytes=8 << 30, max_slots=2)
+    assert [m.done for m in srv2.running] == [10, 10]
+    srv2.run()
+    assert set(srv2.done) == set(specs)
+    for rid, (c, d) in specs.items():
+        assert "error" not in srv2.done[rid], rid
+        assert rel(srv2.done[rid]["ez"], solo_ez(c, d)) < 1e-9, rid

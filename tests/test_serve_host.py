@@ -168,3 +168,12 @@ def test_failing_requests_are_isolated(fake):
     for rid in ("ok", "ok2"):
         assert "error" not in srv.done[rid] and srv.done[rid]["ez"] is not None
     assert srv.used == 0
+
+
+def test_driver_records_round_trip():
+    """Slot files store drivers as JSON; both kinds come back equal."""
+    for d in (batch.GaussianDriver(0.3, 0.8),
+              batch.BeamDriver(n=1234, amplitude=0.2, sigma_r=0.5, seed=9, r_max=1.0)):
+        assert batch.driver_from_record(batch.driver_record(d)) == d
+    with pytest.raises(ValueError):
+        batch.driver_from_record('{"kind": "other"}')
