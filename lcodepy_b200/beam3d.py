@@ -257,12 +257,19 @@ class BeamCalculator:
         self.flags = torch.zeros(stage, dtype=torch.uint8, device=self.device)
 
     def start_time_step(self, source: "BeamSource"):
-        """Zero the planes and counters and lay out the first layer."""
+        """Zero the planes and counters (the first layer is laid out by
+        layout_first).  A streaming source (pipeline.StreamingSource) gives
+        its layer slices as its chunks arrive; its buffers are sized for the
+        whole beam."""
         self.source = source
         self._step_args_cache = {}
-        self.bounds = source.all_layer_bounds()
         n = source.beam.size
-        max_layer = max((b - a for a, b in self.bounds.values()), default=0)
+        if getattr(source, "streaming", False):
+            self.bounds = None
+            max_layer = n
+        else:
+            self.bounds = source.all_layer_bounds()
+            max_layer = max((b - a for a, b in self.bounds.values()), default=0)
         self._ensure(n, max_layer)
         self.planes.zero_()
         self.counts.zero_()
@@ -270,6 +277,8 @@ class BeamCalculator:
         self.fell_cur = 0
 
     def layer_bounds(self, i):
+        if self.bounds is None:
+            return self.source.layer_bounds(i) if i >= 0 else (0, 0)
         return self.bounds.get(i, (0, 0))
 
     def rho(self, i):

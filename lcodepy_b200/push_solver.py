@@ -69,6 +69,9 @@ class PusherAndSolver3D:
             if not self.rigid:
                 # push layer i-1 between the previous and new fields, lay out i+1
                 bc.after_plasma_step(xi_i, ps.last_fields, ps.prev_fields)
+                stream_out = getattr(beam_drain, "after_xi_step", None)
+                if stream_out is not None:    # a pipelined run streams its drain
+                    stream_out(xi_i, bc)
             if diagnostics_list:
                 xi_layer = -self.xi_step_size * xi_i
                 rho = rb_full / bc.rho_divisor
@@ -90,6 +93,8 @@ class PusherAndSolver3D:
                                    "buffer would overflow")
             moved, self.lost = bc.finish()
             beam_drain.push_beam_layer(moved)
+            if getattr(beam_source, "streaming", False):
+                beam_source.finish()
         self.ez_axis = hist[:n_iter].clone()
         ez = self.ez_axis
         if self.print_every:

@@ -4,6 +4,11 @@
 Everything runs on the current CUDA device: the config key
 'processing-unit-type' is accepted for compatibility but this package has no
 CPU path, and it raises if CUDA is unavailable or liblcb.so is missing.
+
+When torch.distributed is initialised with more than one rank, ``step``
+runs the reference's time-step pipeline (lcode/simulation.py:222-264 with
+lcode/mpi/beam_io.py): rank r computes the time steps r, r + W, ... and
+streams its moved beam to the next rank during its xi loop (pipeline.py).
 """
 from __future__ import annotations
 
@@ -111,19 +116,59 @@ class Simulation:
         if self.external_plasmastate:
             from .plasma_state import load_plasmastate
             state = load_plasmastate(self.path_to_plasmastate, ps.plasma_solver.sort_names)
-        self.current_time = self.__time_step_size
-        for t_i in range(N_steps):
+
+        def one_time_step(source, drain):
             ps.plasma_solver.init_state(self.current_time)
             xi_start = self.__config.getfloat('xi-step')
             if state is not None:
                 xs = ps.plasma_solver.load_state(state)
                 if xs is not None:
                     xi_start = xs
-            ps.step_dt(xi_start, self.beam_source, self.beam_drain,
-                       self.current_time, self.diagnostics_list)
+            ps.step_dt(xi_start, source, drain, self.current_time, self.diagnostics_list)
+
+        world, rank = 1, 0
+        if torch.distributed.is_available() and torch.distributed.is_initialized():
+            world, rank = torch.distributed.get_world_size(), torch.distributed.get_rank()
+        if world > 1:
+            self.__step_pipelined(N_steps, world, rank, one_time_step)
+            print('The work is done!')
+            return
+        self.current_time = self.__time_step_size
+        for t_i in range(N_steps):
+            one_time_step(self.beam_source, self.beam_drain)
             if t_i != N_steps - 1 and not self.__rigid_beam:
                 self.beam_source = BeamSource(self.__config, self.beam_drain.beam_slice(),
                                               self.device)
                 self.beam_drain = BeamDrain(self.__config, self.device)
             self.current_time = self.current_time + self.__time_step_size
         print('The work is done!')
+
+    def __step_pipelined(self, N_steps, world, rank, one_time_step):
+        """Time steps rank, rank + world, ... of N_steps (mpi/transport.py:
+        50-52); the beam of time step t comes streamed from the rank that
+        computed t - 1 and goes streamed to the rank that computes t + 1
+        (pipeline.py).  The rank that computes the last time step keeps its
+        moved beam in ``beam_drain``; a rigid driver is one time step, on
+        rank 0."""
+        from .pipeline import BeamTransport, StreamingDrain, StreamingSource, steps_of_rank
+        mine = steps_of_rank(N_steps, rank, world)
+        self.current_time = self.__time_step_size * (rank + 1)   # simulation.py:244
+        if self.__rigid_beam:
+            for _ in mine:
+                one_time_step(self.beam_source, self.beam_drain)
+                self.current_time += self.__time_step_size * world
+            return
+        transport = BeamTransport(self.device)
+        capacity = self.beam_source.beam.size
+        chunk = int(self.__config.getraw('pipeline-chunk-steps') or 32)
+        initial = self.beam_source
+        for t in mine:
+            source = (initial if t == 0 else
+                      StreamingSource(self.__config, transport, (rank - 1) % world, capacity))
+            drain = (BeamDrain(self.__config, self.device) if t == N_steps - 1 else
+                     StreamingDrain(self.__config, transport, (rank + 1) % world, chunk,
+                                    self.device))
+            one_time_step(source, drain)
+            self.beam_source, self.beam_drain = source, drain
+            self.current_time += self.__time_step_size * world
+        transport.wait()

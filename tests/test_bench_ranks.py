@@ -34,7 +34,7 @@ def _rank(rank, ws, port, out):
 
 def test_two_rank_max_over_ranks_and_barrier():
     ws, port = 2, _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_rank, args=(ws, port, out), nprocs=ws, join=True)
         assert dict(out) == {0: 2.5, 1: 2.5}
