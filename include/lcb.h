@@ -327,6 +327,39 @@ int lcb_rigid_gaussian(int grid_steps, double h, double xi_step, double amplitud
 int lcb_record_axis(const double *plane, int grid_steps, int64_t *counter,
                     double *history, int64_t capacity, void *stream);
 
+/* ---------------------------------------------------------------------
+ * Declustering noise filter of the plasma electrons
+ * (lcode/plasma3d/noise_filter.py:82-239; applied after the last move of an
+ * xi step, lcode/plasma3d/solver.py:68-72).  n is the electrons' lattice
+ * side; every array is n x n FP64, C order.
+ * ------------------------------------------------------------------- */
+
+/* dx_inhom, dy_inhom = the mean over the two lattice directions of the
+ * offsets' inhomogeneity (a point minus the mean of its neighbours,
+ * one-sided second differences at the ends, 0 where a stencil offset is
+ * exactly 0): noise_filter.py:52-73, 123-124. */
+int lcb_declustering_inhomogeneity(int n, const double *x_offt, const double *y_offt,
+                                   double *dx_inhom, double *dy_inhom, void *stream);
+
+typedef struct lcb_declustering_args {
+    int n;
+    double xi_step;
+    double force;                      /* declustering-force */
+    double damping;                    /* damping-declustering */
+    double limit;                      /* declustering-limit */
+    const double *dx_inhom, *dy_inhom;         /* lcb_declustering_inhomogeneity */
+    const double *dx_average, *dy_average;     /* their Gaussian averages */
+    const double *dx_chaotic_prev, *dy_chaotic_prev;  /* previous xi step's */
+    double *px, *py;                   /* updated in place */
+    double *dx_chaotic, *dy_chaotic;   /* written (not the previous arrays) */
+} lcb_declustering_args;
+
+/* Chaotic displacement = inhomogeneity - average; limiter 1 - d^2/limit^2
+ * (0 beyond limit); restoring force -force * chaotic * limiter; momentum
+ * kicks to each point and its lattice neighbours and damping of the change
+ * of the chaotic displacement (noise_filter.py:164-232). */
+int lcb_declustering_apply(const lcb_declustering_args *a, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

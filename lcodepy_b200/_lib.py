@@ -85,6 +85,14 @@ class ComputeFieldsArgs(C.Structure):
         ("workspace", _vp), ("workspace_bytes", C.c_size_t)]
 
 
+class DeclusteringArgs(C.Structure):
+    _fields_ = [
+        ("n", _i), ("xi_step", _d), ("force", _d), ("damping", _d), ("limit", _d),
+        ("dx_inhom", _vp), ("dy_inhom", _vp), ("dx_average", _vp), ("dy_average", _vp),
+        ("dx_chaotic_prev", _vp), ("dy_chaotic_prev", _vp), ("px", _vp), ("py", _vp),
+        ("dx_chaotic", _vp), ("dy_chaotic", _vp)]
+
+
 _SIGS = {
     "lcb_last_error": (C.c_char_p, []),
     "lcb_version": (_i, []),
@@ -106,6 +114,8 @@ _SIGS = {
     "lcb_beam_step": (_i, [C.POINTER(BeamStepArgs), _vp]),
     "lcb_rigid_gaussian": (_i, [_i, _d, _d, _d, _d, _d, _i64, _vp, _vp, _vp, _vp]),
     "lcb_record_axis": (_i, [_vp, _i, _vp, _vp, _i64, _vp]),
+    "lcb_declustering_inhomogeneity": (_i, [_i, _vp, _vp, _vp, _vp, _vp]),
+    "lcb_declustering_apply": (_i, [C.POINTER(DeclusteringArgs), _vp]),
     "lcb_beam_move": (_i, [_i64, _d, _d, _i64, _d, _i, _vp, _vp,
                            C.POINTER(Fields7), C.POINTER(Fields7)] + [_vp] * 9 + [_vp, _vp]),
 }

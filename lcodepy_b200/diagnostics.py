@@ -173,11 +173,6 @@ class FXiDiag(Diagnostic):
         self._data['xi'] = []
         self._first = _rank0()
         _check_pictures(output_type)
-        chaotic = (FXiType.dx_chaotic | FXiType.dy_chaotic | FXiType.dx_chaotic_perp |
-                   FXiType.dy_chaotic_perp)
-        if f_xi & chaotic:
-            raise NotImplementedError("the chaotic-displacement quantities belong to the "
-                                      "noise filter, which this package does not build")
 
     def pull_config(self, config):
         self._h = config.getfloat('transverse-step')
@@ -230,6 +225,20 @@ class FXiDiag(Diagnostic):
             d['Phi'].append(self._probe(_t(plasma_fields.Phi)))
         if f & FXiType.Sf:
             d['Sf'].append(_energy_flux(self._h, plasma_particles, plasma_fields))
+        # the declustering filter's chaotic displacements of the electrons:
+        # the largest |value| over the lattice, and over its central two
+        # thirds for the "perp" quantities (Strategy3D.py:85-96, which reads
+        # the same arrays for both)
+        for flag, name, central in ((FXiType.dx_chaotic, 'dx', False),
+                                    (FXiType.dy_chaotic, 'dy', False),
+                                    (FXiType.dx_chaotic_perp, 'dx', True),
+                                    (FXiType.dy_chaotic_perp, 'dy', True)):
+            if f & flag:
+                a = _t(getattr(plasma_particles['electrons'], f'{name}_chaotic'))
+                if central:
+                    a1 = int(a.shape[0] / 6)
+                    a = a[a1:5 * a1, a1:5 * a1]
+                d[f'{name}_chaotic' + ('_perp' if central else '')].append(a.abs().max())
         d['xi'].append(xi_plasma_layer)
 
     def dump(self, current_time, xi_plasma_layer, plasma_particles, plasma_fields,

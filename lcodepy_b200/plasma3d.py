@@ -232,6 +232,9 @@ class PlasmaState:
         n = n_sorts * self.n_per_sort
         self.t = {k: torch.zeros(n, dtype=torch.float64, device=device)
                   for k in PARTICLE_NAMES}
+        # dx_chaotic, dy_chaotic of the first sort (the electrons): the
+        # declustering filter's state, zero while it is off
+        self.chaos = torch.zeros(2, self.n_per_sort, dtype=torch.float64, device=device)
 
     def __getattr__(self, k):
         t = self.__dict__.get("t")
@@ -244,7 +247,9 @@ class PlasmaState:
         a, b = s * self.n_per_sort, (s + 1) * self.n_per_sort
         views = {k: v[a:b].view(self.Ns, self.Ns) for k, v in self.t.items()}
         z = torch.zeros_like(views["x_init"])
-        return Arrays(torch, **views, dx_chaotic=z, dy_chaotic=z,
+        dx, dy = ((self.chaos[0].view(self.Ns, self.Ns), self.chaos[1].view(self.Ns, self.Ns))
+                  if s == 0 else (z, z))
+        return Arrays(torch, **views, dx_chaotic=dx, dy_chaotic=dy,
                       dx_chaotic_perp=z, dy_chaotic_perp=z)
 
 

@@ -26,6 +26,8 @@ CONFIG = {'geometry': '3d', 'processing-unit-type': 'cpu', 'window-width': 1.6,
 CASES = [
     # every FXi quantity but the noise filter's chaotic displacements
     ('fxi_axis', 'FXiDiag', dict(output_period=1, f_xi=0x7ff, directory_name='fa')),
+    # the noise filter's chaotic displacements (whole lattice and centre)
+    ('fxi_chaotic', 'FXiDiag', dict(output_period=1, f_xi=0x4 | 0x7800, directory_name='fc')),
     ('fxi_lines', 'FXiDiag', dict(output_period=1, f_xi=0x4 | 0x80 | 0x200,
                                   probe_lines=[[0.0, 0.2, -0.35], [0.1, 0.0, 0.05]],
                                   directory_name='fl')),
@@ -42,6 +44,9 @@ CASES = [
     ('particles', 'ParticlesDiag', dict(save_beam=True, save_plasma=True, output_period=1,
                                         saving_xi_period=0.2, directory_name='pd')),
 ]
+
+
+PARTICLE_KEYS = ('m', 'px', 'py', 'pz', 'dx_chaotic', 'dy_chaotic')
 
 
 class StubDrain:
@@ -62,8 +67,11 @@ def walk(root):
 def diag_steps(N, n_steps=11, times=(0.0, 1.0, 2.0), dxi=0.05, seed=77):
     """Seeded synthetic inputs: for each time and xi step, a dict of host
     arrays (fields Ex..Bz, Phi; currents ro (2, N, N); electrons m, px, py,
-    pz (20 x 20); rho_beam)."""
+    pz, dx_chaotic, dy_chaotic (20 x 20); rho_beam).  The chaotic
+    displacements come from a second stream, so the other inputs do not
+    depend on them."""
     rng = np.random.default_rng(seed)
+    rng_c = np.random.default_rng(seed + 1)
     out = []
     for t in times:
         for k in range(n_steps):
@@ -73,6 +81,8 @@ def diag_steps(N, n_steps=11, times=(0.0, 1.0, 2.0), dxi=0.05, seed=77):
             f['m'] = np.full((20, 20), 0.0025)
             for n in ('px', 'py', 'pz'):
                 f[n] = rng.standard_normal((20, 20)) * 0.01
+            for n in ('dx_chaotic', 'dy_chaotic'):
+                f[n] = rng_c.standard_normal((20, 20)) * 1e-3
             out.append((t, -k * dxi, f))
     return out
 
@@ -107,7 +117,7 @@ def main(ref_root):
                     last_t = t
                     fields = Arrays(np, **{n: f[n] for n in ('Ex', 'Ey', 'Ez', 'Bx', 'By', 'Bz', 'Phi')})
                     currents = Arrays(np, ro=f['ro'])
-                    particles = {'electrons': Arrays(np, m=f['m'], px=f['px'], py=f['py'], pz=f['pz'])}
+                    particles = {'electrons': Arrays(np, **{n: f[n] for n in PARTICLE_KEYS})}
                     d.after_step_dxi(t, xi, particles, fields, currents, f['rho_beam'])
                 d.dump(last_t, 0.0, particles, None, None, drain)
                 sub = os.path.join(td, 'diagnostics', kw['directory_name'])
@@ -122,4 +132,6 @@ def main(ref_root):
 
 
 if __name__ == '__main__':
-    main(sys.argv[1] if len(sys.argv) > 1 else '/path/to/lcodePy')
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from oracle.ref_kernels import reference_root
+    main(sys.argv[1] if len(sys.argv) > 1 else reference_root())

@@ -14,7 +14,7 @@ torch = pytest.importorskip("torch")
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(HERE, "golden"))
-from make_diag_golden import CASES, CONFIG, StubDrain, diag_steps, walk  # noqa: E402
+from make_diag_golden import CASES, CONFIG, PARTICLE_KEYS, StubDrain, diag_steps, walk  # noqa: E402
 
 from lcodepy_b200 import diagnostics as D  # noqa: E402
 from lcodepy_b200.config import Config  # noqa: E402
@@ -53,7 +53,7 @@ def test_diagnostic_files_match_reference(tmp_path, monkeypatch, case, cls, kw, 
         currents = _ns(dev, ro=f['ro'])
         # what the drop-in Simulation hands to diagnostics: wrapped Arrays
         particles = {'electrons': Arrays(torch, **{n: torch.as_tensor(f[n], device=dev)
-                                                   for n in ('m', 'px', 'py', 'pz')}).wrapped()}
+                                                   for n in PARTICLE_KEYS}).wrapped()}
         d.after_step_dxi(t, xi, particles, fields, currents,
                          DeviceArray(torch.as_tensor(f['rho_beam'], device=dev)))
     d.dump(last_t, 0.0, particles, None, None, drain)
@@ -71,8 +71,3 @@ def test_diagnostic_files_match_reference(tmp_path, monkeypatch, case, cls, kw, 
                     np.testing.assert_allclose(z[k], ref, rtol=1e-12)
                 else:
                     np.testing.assert_array_equal(z[k], ref)
-
-
-def test_chaotic_quantities_are_refused():
-    with pytest.raises(NotImplementedError):
-        D.FXiDiag(f_xi=D.FXiType.dx_chaotic)

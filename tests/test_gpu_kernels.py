@@ -237,6 +237,44 @@ def test_fused_stage_forms_match_separate_kernels(precision):
         np.testing.assert_array_equal(runs[1][1], fus_c)
 
 
+def test_declustering_filter_vs_reference(golden):
+    """The noise filter's two kernels with the Gaussian average between them
+    (cuFFT) against the reference's filter applied to the same seeded
+    electron arrays (kat_noise_filter.npz)."""
+    d = golden("kat_noise_filter.npz")
+    L = _lib.load()
+    n = d["x_offt"].shape[0]
+    st = _lib.stream_handle()
+    b = torch.zeros(4, n, n, dtype=torch.float64, device=DEV)
+    xo, yo = T(d["x_offt"]), T(d["y_offt"])
+    _lib.check(L.lcb_declustering_inhomogeneity(n, xo.data_ptr(), yo.data_ptr(),
+                                                b[0].data_ptr(), b[1].data_ptr(), st), "inhom")
+    f = torch.fft.fftfreq(n, dtype=torch.float64, device=DEV)
+    g = torch.exp(-2 * np.pi ** 2 * float(d["declustering_averaging"]) ** 2 * f * f)
+    b[2:4].copy_(torch.fft.ifft2(torch.fft.fft2(b[0:2]) * (g[:, None] * g[None, :])).real)
+    px, py = T(d["px"]), T(d["py"])
+    px0, py0 = px.clone(), py.clone()
+    prev = [T(d["dx_chaotic_prev"]), T(d["dy_chaotic_prev"])]
+    out = [torch.zeros(n, n, dtype=torch.float64, device=DEV) for _ in range(2)]
+    a = _lib.DeclusteringArgs()
+    a.n, a.xi_step = n, float(d["dxi"])
+    a.force, a.damping = float(d["declustering_force"]), float(d["damping_declustering"])
+    a.limit = float(d["declustering_limit"])
+    a.dx_inhom, a.dy_inhom, a.dx_average, a.dy_average = (b[k].data_ptr() for k in range(4))
+    a.dx_chaotic_prev, a.dy_chaotic_prev = prev[0].data_ptr(), prev[1].data_ptr()
+    a.px, a.py = px.data_ptr(), py.data_ptr()
+    a.dx_chaotic, a.dy_chaotic = out[0].data_ptr(), out[1].data_ptr()
+    _lib.check(L.lcb_declustering_apply(C.byref(a), st), "apply")
+    torch.cuda.synchronize()
+    close(N_(out[0]), d["out_dx_chaotic"], 1e-12, "dx_chaotic")
+    close(N_(out[1]), d["out_dy_chaotic"], 1e-12, "dy_chaotic")
+    close(N_(px), d["out_px"], 1e-12, "px")
+    close(N_(py), d["out_py"], 1e-12, "py")
+    # the kicks themselves (a small change of px, py), to 1e-9 of their size
+    close(N_(px - px0), d["out_px"] - d["px"], 1e-9, "px kick")
+    close(N_(py - py0), d["out_py"] - d["py"], 1e-9, "py kick")
+
+
 def _fields_args(d, precision, ops, outs, ws):
     N = int(d["N"])
     keep = []

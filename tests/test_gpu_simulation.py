@@ -74,6 +74,29 @@ def test_rigid_vs_reference(golden, fixture, extra, sorts):
     check(ref, particles, fields, currents, sorts, 1e-8)
 
 
+def test_declustering_vs_reference(golden):
+    """The declustering noise filter on (noise_filter.py:82-239; the
+    reference reads 'damping-declustering') over 21 xi steps of the rigid
+    configuration, against the reference's run.  With the filter on, this
+    configuration amplifies rounding differences about tenfold every 1.5 xi
+    steps (measured), so after 21 steps the electrons' momenta, where the
+    filter's kicks act, agree to 1e-6 of their largest value; on-axis Ez,
+    fields and currents to 1e-9 / 1e-8."""
+    ref = golden("run_declustering.npz")
+    extra = {'window-length': 1.0, 'declustering-enabled': True,
+             'declustering-averaging': 3, 'declustering-force': 0.3,
+             'damping-declustering': 0.1, 'declustering-limit': 2e-3}
+    _, particles, fields, currents, ez = run(cfg(**{'rigid-beam': True, **extra}), rigid_driver)
+    assert rel_err(ez, ref["ez_axis"]) < 1e-9
+    for k in ("Ex", "Ey", "Ez", "Bx", "By", "Bz", "Phi"):
+        assert rel_err(getattr(fields, k).cpu().numpy(), ref["f_" + k]) < 1e-8, k
+    for k in ("ro", "jx", "jy", "jz"):
+        assert rel_err(getattr(currents, k).cpu().numpy(), ref["c_" + k]) < 1e-8, k
+    for k in ("x_offt", "y_offt", "px", "py", "pz", "q"):
+        e = rel_err(getattr(particles["electrons"], k).cpu().numpy(), ref["p_electrons_" + k])
+        assert e < 1e-6, (k, e)
+
+
 def test_generated_beam_vs_reference(golden):
     ref = golden("run_beam.npz")
     _, particles, fields, currents, ez = run(

@@ -52,3 +52,21 @@ def test_generator_matches_reference(golden):
         assert got.dtype == ref.dtype and got.shape == ref.shape
         for k in ref.dtype.names:
             np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
+
+
+def test_declustering_average_is_scipys_fourier_gaussian():
+    """The solver averages the inhomogeneity by multiplying its FFT with
+    exp(-2 pi^2 sigma^2 f^2) per axis (f the FFT frequencies); that is
+    scipy.ndimage.fourier_gaussian, which the reference calls
+    (noise_filter.py:142-143), for odd and even lattice sides."""
+    import numpy as np
+    import torch
+    from scipy.ndimage import fourier_gaussian
+    rng = np.random.default_rng(5)
+    for n, sigma in ((40, 3.0), (33, 1.5)):
+        a = rng.normal(size=(n, n))
+        want = np.fft.ifft2(fourier_gaussian(np.fft.fft2(a), sigma=sigma)).real
+        f = torch.fft.fftfreq(n, dtype=torch.float64)
+        g = torch.exp(-2 * np.pi ** 2 * sigma ** 2 * f * f)
+        got = torch.fft.ifft2(torch.fft.fft2(torch.tensor(a)) * (g[:, None] * g[None, :])).real
+        assert np.abs(got.numpy() - want).max() < 1e-14 * np.abs(want).max()
