@@ -244,7 +244,8 @@ def run_rigid129(args, ws, rank, local):
            'print-every': 0, 'precision': args.precision}
     times = []
     for rep in range(args.warmup + args.steps):
-        sim = Simulation(config=cfg, beam_parameters=rigid_driver, runas_filename='')
+        sim = Simulation(config={**cfg, 'time-step-pipeline': False},
+                         beam_parameters=rigid_driver, runas_filename='')
         ps = sim.push_solver
         ev = {}
 
@@ -366,7 +367,7 @@ def run_plain_requests(reqs, dev, extra=None):
     out = {}
     with tempfile.TemporaryDirectory() as td:
         for arr, rid, cfg, drv in reqs:
-            c = {**cfg, 'precision': 'fp64', **(extra or {})}
+            c = {**cfg, 'precision': 'fp64', 'time-step-pipeline': False, **(extra or {})}
             path = None
             if isinstance(drv, BeamDriver):
                 c['rigid-beam'] = False
@@ -500,7 +501,9 @@ def run_e2e(cfg, beam_host, dev):
     with tempfile.TemporaryDirectory() as td:
         path = os.path.join(td, "beam.npz")
         np.savez(path, **{k: beam_host[k] for k in beam_host.dtype.names})
-        sim = Simulation(config=cfg, beam_parameters={}, runas_filename='')
+        # every rank is an independent replica, not a time-step pipeline stage
+        sim = Simulation(config={**cfg, 'time-step-pipeline': False}, beam_parameters={},
+                         runas_filename='')
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         sim.load_beamfile(path)

@@ -127,7 +127,11 @@ class Simulation:
             ps.step_dt(xi_start, source, drain, self.current_time, self.diagnostics_list)
 
         world, rank = 1, 0
-        if torch.distributed.is_available() and torch.distributed.is_initialized():
+        # 'time-step-pipeline': False keeps every rank an independent replica
+        # (a process group set up for something else, e.g. timing replicas)
+        pipe = self.__config.getraw('time-step-pipeline')
+        if (torch.distributed.is_available() and torch.distributed.is_initialized()
+                and (pipe is None or bool(pipe))):
             world, rank = torch.distributed.get_world_size(), torch.distributed.get_rank()
         if world > 1:
             self.__step_pipelined(N_steps, world, rank, one_time_step)
