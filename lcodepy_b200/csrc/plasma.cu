@@ -835,8 +835,8 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
         zero_p[p] = z;
         double xl, yl;
         // FP64: the quotient of K2 itself; mixed: the reciprocal
-        ix[p] = cell_of((MIXED ? xh * ih : xh / h) + 0.5, half_n, xl);
-        iy[p] = cell_of((MIXED ? yh * ih : yh / h) + 0.5, half_n, yl);
+        ix[p] = cell_of(xh * ih + 0.5, half_n, xl);
+        iy[p] = cell_of(yh * ih + 0.5, half_n, yl);
         xlf[p] = (FT)xl; ylf[p] = (FT)yl;
         if (!(ix[p] >= 2 && ix[p] < N - 2 && iy[p] >= 2 && iy[p] < N - 2)) {
             if (err) atomicOr(err, LCB_DEVERR_PLASMA_STENCIL);
@@ -995,21 +995,13 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
 #pragma unroll
         for (int it = 0; it < 2; it++) {
             gm = sqrt(mk * mk + px * px + py * py + pz * pz);
-            if (MIXED) {
-                // f (E + v x B) with v = p / gm and f = q dxi / (1 - vz),
-                // as q dxi (gm E + p x B) / (gm - pz): one quotient
-                const double r = qk * xi_step / (gm - pz);
-                dpx = r * (gm * Ex + py * Bz - pz * By);
-                dpy = r * (gm * Ey - px * Bz + pz * Bx);
-                dpz = r * (gm * Ez + px * By - py * Bx);
-            } else {
-                const double ig = 1.0 / gm;
-                const double vx = px * ig, vy = py * ig, vz = pz * ig;
-                const double f = qk * xi_step / (1 - vz);
-                dpx = f * (Ex + vy * Bz - vz * By);
-                dpy = f * (Ey - vx * Bz + vz * Bx);
-                dpz = f * (Ez + vx * By - vy * Bx);
-            }
+            // f (E + v x B) with v = p / gm and f = q dxi / (1 - vz), as
+            // q dxi (gm E + p x B) / (gm - pz): one quotient (algebraically
+            // the reference's two, move.py:234-239)
+            const double r = qk * xi_step / (gm - pz);
+            dpx = r * (gm * Ex + py * Bz - pz * By);
+            dpy = r * (gm * Ey - px * Bz + pz * Bx);
+            dpz = r * (gm * Ez + px * By - py * Bx);
             px = opx + dpx * 0.5; py = opy + dpy * 0.5; pz = opz + dpz * 0.5;
         }
         gm = sqrt(mk * mk + px * px + py * py + pz * pz);
@@ -1032,20 +1024,13 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
         if (FIRST || absorbed) q_f[k] = absorbed ? 0.0 : qk;
         if (absorbed) continue;
         const double gd = sqrt(mk * mk + px * px + py * py + pz * pz);
-        double dro, djx, djy, djz;
-        if (MIXED) {
-            // q / (1 - pz / gd) and p q / (gd - pz): one quotient
-            const double r = qk / (gd - pz);
-            dro = r * gd; djx = r * px; djy = r * py; djz = r * pz;
-        } else {
-            const double igd = 1.0 / gd;
-            dro = qk / (1 - pz * igd);
-            const double rg = dro * igd;
-            djx = px * rg; djy = py * rg; djz = pz * rg;
-        }
+        // q / (1 - pz / gd) and p q / (gd - pz): one quotient (weights.py:
+        // 164-168 has two)
+        const double r = qk / (gd - pz);
+        const double dro = r * gd, djx = r * px, djy = r * py, djz = r * pz;
         if (MIXED) check_range<fix_t>(dro, djx, djy, djz, ih, err);
-        const int c_x = cell_of((MIXED ? (xi0 + xo) * ih : (xi0 + xo) / h) + 0.5, half_n, dxl[p]);
-        const int c_y = cell_of((MIXED ? (yi0 + yo) * ih : (yi0 + yo) / h) + 0.5, half_n, dyl[p]);
+        const int c_x = cell_of((xi0 + xo) * ih + 0.5, half_n, dxl[p]);
+        const int c_y = cell_of((yi0 + yo) * ih + 0.5, half_n, dyl[p]);
         if (!(c_x >= 2 && c_x < N - 2 && c_y >= 2 && c_y < N - 2)) {
             if (err) atomicOr(err, LCB_DEVERR_PLASMA_STENCIL);
             continue;
