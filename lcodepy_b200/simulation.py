@@ -162,6 +162,9 @@ class Simulation:
                 one_time_step(self.beam_source, self.beam_drain)
                 self.current_time += self.__time_step_size * world
             return
+        if getattr(self.beam_source, "streaming", False):
+            raise NotImplementedError("a pipelined run is one step() call; start a new "
+                                      "Simulation for the next one")
         transport = BeamTransport(self.device)
         capacity = self.beam_source.beam.size
         chunk = int(self.__config.getraw('pipeline-chunk-steps') or 32)
