@@ -783,7 +783,7 @@ def main():
 # fused stage averaged over the xi step's three stages (+ the fixed-point
 # finish in mixed precision).
 NCU_TRAFFIC = {("compute_fields", "fp64"): 197.9e6, ("compute_fields", "mixed"): 128.2e6,
-               ("move_deposit", "fp64"): 111.4e6, ("move_deposit", "mixed"): 125.4e6}
+               ("move_deposit", "fp64"): 110.8e6, ("move_deposit", "mixed"): 125.7e6}
 
 # algorithmic bytes per plasma particle and xi step: K1 64 B (read m, px, py,
 # pz, x_offt, y_offt; write x_offt, y_offt) + 3 x K2 128 B (read 11 x 8 B,
