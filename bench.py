@@ -173,6 +173,7 @@ def run_gpu(args, ws, rank, local):
     torch.cuda.synchronize()
     ev = {}
     op_times = {}
+    op_marks = []     # (xi step, per-op launch counts before it): --op-timeline
 
     def hook(k):
         if k == W:
@@ -185,7 +186,10 @@ def run_gpu(args, ws, rank, local):
         if W <= k < W + K:
             # every 16th timed step runs eagerly with per-op CUDA events (the
             # kernels are the same; the others replay the captured graphs)
-            ps.plasma_solver.op_timers = op_times if (k - W) % 16 == 0 else None
+            every = args.op_every
+            ps.plasma_solver.op_timers = op_times if (k - W) % every == 0 else None
+            if (k - W) % every == 0:
+                op_marks.append((k, {n: len(v) for n, v in op_times.items()}))
         if k == W + K:
             ev["t1"] = torch.cuda.Event(enable_timing=True)
             ev["t1"].record()
@@ -210,6 +214,16 @@ def run_gpu(args, ws, rank, local):
     for name, evs in op_times.items():
         tot = sum(a.elapsed_time(b) for a, b in evs)
         ops[name] = {"launches": len(evs), "ms_total": tot, "ms_avg": tot / max(len(evs), 1)}
+    if args.op_timeline and rank == 0:
+        # per eagerly timed xi step: each op's launches, in microseconds
+        line = {}
+        ends = op_marks[1:] + [(None, {n: len(v) for n, v in op_times.items()})]
+        for (k, a), (_, b) in zip(op_marks, ends):
+            line[k] = {n: [round(e0.elapsed_time(e1) * 1e3, 1)
+                           for e0, e1 in op_times[n][a.get(n, 0):b.get(n, 0)]]
+                       for n in op_times}
+        with open(args.op_timeline, "w") as f:
+            json.dump(line, f)
 
     # ---- end to end through the public API, host buffers in and out ----
     e2e = None if args.no_e2e else run_e2e(cfg, beam_host, dev)
@@ -634,12 +648,19 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the end-to-end Simulation run (profiling runs)")
+    ap.add_argument("--op-every", type=int, default=16,
+                    help="per-op CUDA events on every K-th timed xi step (run eagerly)")
+    ap.add_argument("--op-timeline", default=None,
+                    help="write each eagerly timed xi step's per-op launch times (us) "
+                         "to this JSON file")
     ap.add_argument("--window-length", type=float, default=60.0,
                     help="xi window length; smaller values give the small "
                          "profiling case of the same grid and beam")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
+    if args.op_every < 1:
+        raise SystemExit("--op-every must be >= 1")
     ws, rank, local = dist_init()
 
     if args.impl == "reference":
