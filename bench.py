@@ -572,7 +572,8 @@ def run_headline(args, ws, rank, local):
             "workload": f"served stream: {args.requests} requests (Poisson 20/s, seeded), grids "
                         "129/257/513 at h=0.05, 200-2000 xi steps of 0.05, half rigid "
                         "Gaussian, half bi-Gaussian beams of 100k-1M macroparticles",
-            "precision": "mixed", "value": v["value"], "unit": METRIC,
+            "precision": "mixed", "slots": args.slots, "hbm_budget_gb": args.hbm_budget_gb,
+            "value": v["value"], "unit": METRIC,
             "latency_s": {"p50": v["p50"], "p99": v["p99"]},
             "plain_fp64": {"value": v["plain_value"], "p50": v["plain_p50"],
                            "p99": v["plain_p99"], "busy_s": v["plain_busy_s"],
