@@ -59,9 +59,14 @@ class BeamTransport:
     def _wire(self, t: torch.Tensor) -> torch.Tensor:
         return t.cpu() if self.staged else t
 
+    def _wire_device(self):
+        """Where received tensors land: host memory when staged."""
+        return torch.device("cpu") if self.staged else self.device
+
     def send(self, dst: int, beam: BeamParticles, complete: int, last: bool):
         n = beam.size
-        header = torch.tensor([n, complete, int(last)], dtype=torch.int64, device=self.device)
+        header = torch.tensor([n, complete, int(last)], dtype=torch.int64,
+                              device=self._wire_device())
         cols = []
         for k in _keys():
             a = getattr(beam, k)
@@ -76,14 +81,13 @@ class BeamTransport:
 
     def recv(self, src: int):
         """(BeamParticles on the device, layers complete, last chunk)."""
-        header = self._wire(torch.zeros(3, dtype=torch.int64, device=self.device))
+        header = torch.zeros(3, dtype=torch.int64, device=self._wire_device())
         dist.recv(header, src, group=self.group)
         n, complete, last = (int(v) for v in header.tolist())
         keys = _keys()
         b = BeamParticles(self.device)
         if n:
-            payload = self._wire(torch.empty(len(keys), n, dtype=torch.float64,
-                                             device=self.device))
+            payload = torch.empty(len(keys), n, dtype=torch.float64, device=self._wire_device())
             dist.recv(payload, src, group=self.group)
             payload = payload.to(self.device)
             for j, k in enumerate(keys):
