@@ -288,7 +288,9 @@ class Member:
         os.makedirs(directory, exist_ok=True)
         base = os.path.join(directory, str(self.name if self.name is not None else "member"))
         ps = self.solver
-        save_plasmastate(base + ".plasma.npz", ps.particles_dict(), ps.prev_fields.arrays(),
+        # each file is written under a temporary name and renamed, so that an
+        # interrupted checkpoint leaves the previous files, not truncated ones
+        save_plasmastate(base + ".plasma.tmp.npz", ps.particles_dict(), ps.prev_fields.arrays(),
                          ps.prev_currents.arrays(), ro_initial=ps.ro_initial,
                          xi_plasma_layer=-self.dxi * (self.done - 1))
         meta = {"format": np.array(SLOT_FORMAT), "name": np.array(str(self.name)),
@@ -298,7 +300,9 @@ class Member:
                 "ez": self.ez[:self.done].cpu().numpy(),
                 "arrival": np.array(float(getattr(self, "t_arrival", 0.0) or 0.0))}
         meta.update(self._slot_state())
-        np.savez(base + ".slot.npz", **meta)
+        np.savez(base + ".slot.tmp.npz", **meta)
+        os.replace(base + ".plasma.tmp.npz", base + ".plasma.npz")
+        os.replace(base + ".slot.tmp.npz", base + ".slot.npz")
         return base
 
     def _slot_state(self) -> dict:
@@ -452,6 +456,10 @@ def restore_member(base: str, device=None) -> Member:
     m = make_member(config, driver, device, name=str(meta["name"]))
     state = load_plasmastate(base + ".plasma.npz", m.solver.sort_names)
     done = int(meta["done"])
+    xi = state["xi_plasma_layer"]
+    if xi is None or abs(xi + m.dxi * (done - 1)) > 1e-9 * max(1.0, abs(xi)):
+        raise ValueError(f"{base}: the plasma state (xi {xi}) is not the layer of the "
+                         f"slot file ({done} steps done)")
     with torch.cuda.stream(m.stream):
         m.solver.load_state(state)
         m.counter.fill_(done)
@@ -783,8 +791,10 @@ class Server:
             running.append({"base": os.path.basename(base), "arrival": m.t_arrival - t})
         waiting = [{"id": rid, "config": cfg, "driver": driver_record(drv),
                     "arrival": arr - t} for arr, rid, cfg, drv in self.waiting]
-        with open(os.path.join(directory, "server.json"), "w") as f:
+        path = os.path.join(directory, "server.json")
+        with open(path + ".tmp", "w") as f:
             json.dump({"format": SLOT_FORMAT, "running": running, "waiting": waiting}, f)
+        os.replace(path + ".tmp", path)
 
     @classmethod
     def restore(cls, directory, hbm_budget_bytes: int, max_slots: int = 64, device=None):
