@@ -635,7 +635,7 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--members", type=int, default=64, help="batch: scan members")
     ap.add_argument("--requests", type=int, default=64, help="serve: requests in the stream")
-    ap.add_argument("--slots", type=int, default=48, help="serve: concurrent members")
+    ap.add_argument("--slots", type=int, default=32, help="serve: concurrent members")
     ap.add_argument("--no-plain", action="store_true",
                     help="serve: skip the request-by-request plain FP64 comparison")
     ap.add_argument("--hbm-budget-gb", type=int, default=64, help="serve: HBM admission budget")
