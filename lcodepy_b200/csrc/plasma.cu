@@ -1084,20 +1084,28 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
                                                 dyl[1], sv[1]);
                 }
             } else if (joint) {
+                // the rows of the stencil in a rolled loop (the x weights
+                // move down one register per row): a fifth of the code,
+                // which keeps the stage's hot path within the instruction
+                // cache
                 double ax[5], ay[5], bx[5], by[5];
                 weights4(dxl[0], ax); weights4(dyl[0], ay);
                 weights4(dxl[1], bx); weights4(dyl[1], by);
-#pragma unroll
+                int row = lx * WY + ly;
+#pragma unroll 1
                 for (int a = 0; a < 5; a++) {
+                    const double xa = ax[0], xb = bx[0];
 #pragma unroll
                     for (int b = 0; b < 5; b++) {
-                        const double wa = ax[a] * ay[b], wb = bx[a] * by[b];
-                        const int c = (lx + a) * WY + ly + b;
+                        const double wa = xa * ay[b], wb = xb * by[b];
 #pragma unroll
                         for (int q = 0; q < 4; q++)
-                            shared_fix_add(swl, swh, q * WSZ + c,
+                            shared_fix_add(swl, swh, q * WSZ + row + b,
                                            fma(sv[0][q], wa, fma(sv[1][q], wb, FIX_MAGIC)));
                     }
+#pragma unroll
+                    for (int k = 0; k < 4; k++) { ax[k] = ax[k + 1]; bx[k] = bx[k + 1]; }
+                    row += WY;
                 }
             }
         }
@@ -1138,23 +1146,29 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
                                                   dxl[p], dyl[p], sv[p]);
             }
         } else if (joint && ok) {
-            // the two contributions summed before the fixed-point atomics
+            // the two contributions summed before the fixed-point atomics;
+            // the rows of the stencil in a rolled loop (the x weights move
+            // down one register per row): a fifth of the code, which keeps
+            // the stage's hot path within the instruction cache
             double ax[5], ay[5], bx[5], by[5];
             weights4(dxl[0], ax); weights4(dyl[0], ay);
             weights4(dxl[1], bx); weights4(dyl[1], by);
 #pragma unroll
             for (int b = 0; b < 5; b++) { ay[b] *= ih; by[b] *= ih; }
-#pragma unroll
+            int row = lx * WY + ly;
+#pragma unroll 1
             for (int a = 0; a < 5; a++) {
-                const double xa = ax[a] * ih, xb = bx[a] * ih;
+                const double xa = ax[0] * ih, xb = bx[0] * ih;
 #pragma unroll
                 for (int b = 0; b < 5; b++) {
                     const double wa = xa * ay[b], wb = xb * by[b];
-                    const int c = (lx + a) * WY + ly + b;
 #pragma unroll
                     for (int q = 0; q < 4; q++)
-                        fix56_add(swl, sw1, sw2, q * WSZ + c, fma(sv[0][q], wa, sv[1][q] * wb));
+                        fix56_add(swl, sw1, sw2, q * WSZ + row + b, fma(sv[0][q], wa, sv[1][q] * wb));
                 }
+#pragma unroll
+                for (int k = 0; k < 4; k++) { ax[k] = ax[k + 1]; bx[k] = bx[k + 1]; }
+                row += WY;
             }
         }
     }
