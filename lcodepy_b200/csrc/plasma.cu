@@ -930,13 +930,15 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
             weights4f((float)xlf[0], ax); weights4f((float)ylf[0], ay);
             weights4f((float)xlf[1], bx); weights4f((float)ylf[1], by);
             unsigned long long A[3] = {0ull, 0ull, 0ull}, B[3] = {0ull, 0ull, 0ull};
-#pragma unroll
+            // stencil rows in a rolled loop, as in the deposit
+            int row = lx * WY + ly;
+#pragma unroll 1
             for (int a = 0; a < 5; a++) {
 #pragma unroll
                 for (int b = 0; b < 5; b++) {
-                    const float wa = ax[a] * ay[b], wb = bx[a] * by[b];
+                    const float wa = ax[0] * ay[b], wb = bx[0] * by[b];
                     const unsigned long long wa2 = f32x2(wa, wa), wb2 = f32x2(wb, wb);
-                    const int c = (lx + a) * WY + ly + b;
+                    const int c = row + b;
                     const float4 p = reinterpret_cast<const float4 *>(sf)[c];
                     const float2 q = reinterpret_cast<const float2 *>(sf + 16 * WSZ)[c];
                     const unsigned long long v3[3] = {f32x2(p.x, p.y), f32x2(p.z, p.w), f32x2(q.x, q.y)};
@@ -946,6 +948,9 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
                         B[k] = fma_f32x2(v3[k], wb2, B[k]);
                     }
                 }
+#pragma unroll
+                for (int k = 0; k < 4; k++) { ax[k] = ax[k + 1]; bx[k] = bx[k + 1]; }
+                row += WY;
             }
 #pragma unroll
             for (int k = 0; k < 3; k++) {
@@ -957,19 +962,23 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
             FT ax[5], ay[5], bx[5], by[5];
             weights_of(xlf[0], ax); weights_of(ylf[0], ay);
             weights_of(xlf[1], bx); weights_of(ylf[1], by);
-#pragma unroll
+            int row = lx * WY + ly;
+#pragma unroll 1
             for (int a = 0; a < 5; a++) {
 #pragma unroll
                 for (int b = 0; b < 5; b++) {
-                    const FT wa = ax[a] * ay[b], wb = bx[a] * by[b];
+                    const FT wa = ax[0] * ay[b], wb = bx[0] * by[b];
                     FT v[6];
-                    FieldWin<FT>::get(sf, WSZ, (lx + a) * WY + ly + b, v);
+                    FieldWin<FT>::get(sf, WSZ, row + b, v);
 #pragma unroll
                     for (int f = 0; f < 6; f++) {
                         F0[f] += v[f] * wa;
                         F1[f] += v[f] * wb;
                     }
                 }
+#pragma unroll
+                for (int k = 0; k < 4; k++) { ax[k] = ax[k + 1]; bx[k] = bx[k + 1]; }
+                row += WY;
             }
         }
     }
@@ -1063,17 +1072,20 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
                     weights4(dyl[0], t); shift6(t, cy[0] - mcy, ay);
                     weights4(dxl[1], t); shift6(t, cx[1] - mcx, bx);
                     weights4(dyl[1], t); shift6(t, cy[1] - mcy, by);
-#pragma unroll
+                    int row = dx0 * WY + dy0;
+#pragma unroll 1
                     for (int a = 0; a < 6; a++) {
 #pragma unroll
                         for (int b = 0; b < 6; b++) {
-                            const double wa = ax[a] * ay[b], wb = bx[a] * by[b];
-                            const int c = (dx0 + a) * WY + dy0 + b;
+                            const double wa = ax[0] * ay[b], wb = bx[0] * by[b];
 #pragma unroll
                             for (int q = 0; q < 4; q++)
-                                shared_fix_add(swl, swh, q * WSZ + c,
+                                shared_fix_add(swl, swh, q * WSZ + row + b,
                                                fma(sv[0][q], wa, fma(sv[1][q], wb, FIX_MAGIC)));
                         }
+#pragma unroll
+                        for (int k = 0; k < 5; k++) { ax[k] = ax[k + 1]; bx[k] = bx[k + 1]; }
+                        row += WY;
                     }
                 } else {
                     if (cx[0] >= 0)
@@ -1126,17 +1138,20 @@ k_move_deposit_pair(int64_t n_per_sort, int Ns, int N, double h, double xi_step,
                 weights4(dyl[1], t); shift6(t, cy[1] - mcy, by);
 #pragma unroll
                 for (int b = 0; b < 6; b++) { ay[b] *= ih; by[b] *= ih; }
-#pragma unroll
+                int row = dx0 * WY + dy0;
+#pragma unroll 1
                 for (int a = 0; a < 6; a++) {
-                    const double xa = ax[a] * ih, xb = bx[a] * ih;
+                    const double xa = ax[0] * ih, xb = bx[0] * ih;
 #pragma unroll
                     for (int b = 0; b < 6; b++) {
                         const double wa = xa * ay[b], wb = xb * by[b];
-                        const int c = (dx0 + a) * WY + dy0 + b;
 #pragma unroll
                         for (int q = 0; q < 4; q++)
-                            fix56_add(swl, sw1, sw2, q * WSZ + c, fma(sv[0][q], wa, sv[1][q] * wb));
+                            fix56_add(swl, sw1, sw2, q * WSZ + row + b, fma(sv[0][q], wa, sv[1][q] * wb));
                     }
+#pragma unroll
+                    for (int k = 0; k < 5; k++) { ax[k] = ax[k + 1]; bx[k] = bx[k + 1]; }
+                    row += WY;
                 }
             } else {
 #pragma unroll
